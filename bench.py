@@ -1,0 +1,355 @@
+"""Benchmark: RK4 steps/s of the density-matrix propagator on the 22-orbital
+72x72 HSEX workload (tmd22_rk4), one B200 per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  A step is one RK4 step of every solve in the
+handle (4 right-hand sides + stage updates).  `value` is steps/s summed over
+all solves and ranks (each rank runs its own independent solves: the single
+solve does not shard, so N > 1 runs replicas, weak scaling).
+
+--impl reference times the reference's CPU propagation of the same workload
+on the host cores.  The reference needs MKL/FFTW/MPI, which this image lacks,
+so that arm runs the FP64 CPU restatement in oracle/ (kind "port").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK4 steps/s, 22-band 72x72 HSEX: mixed+batched vs plain FP64 GPU @1e-8"
+WORKLOAD = "tmd22_rk4"
+GRID = (72, 72, 1)
+
+
+def workload_input(cache_dir: str) -> dict:
+    import __graft_entry__ as ge
+
+    pkg = ge.load_package()
+    stamp = os.path.join(cache_dir, "input.json")
+    if os.path.exists(stamp):
+        with open(stamp) as f:
+            return json.load(f)
+    inp = pkg.workloads.make(WORKLOAD, cache_dir, grid=GRID, nsteps=4000)
+    pkg.workloads.save_input(inp, stamp)
+    return inp
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(P, Nk, B, d_E, coulomb=True):
+    """Algorithmic HBM bytes of one RK4 step's launches (FP64, 16 B complex).
+
+    plane kernel, per plane: read rho_s, write G; HSEX adds read rho0, read W
+    (real, 8 B), write Hee.
+    commutator kernel, per element: read rho_s, G, H0, d_E*xi [, Hee] and the
+    stage bookkeeping: RK1 writes aux, acc; RK2/3 read y, acc and write aux,
+    acc; RK4 reads acc and writes y."""
+    c = 16.0
+    plane = P * Nk * ((2 * c) + ((c + 8 + c) if coulomb else 0)) * B
+    common = c * (3 + d_E + (1 if coulomb else 0))
+    comm = [common + 2 * c, common + 4 * c, common + 4 * c, common + 2 * c]
+    comm_total = sum(P * Nk * x for x in comm) * B
+    return plane, comm_total
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    import __graft_entry__ as ge
+
+    pkg = ge.load_package()
+    torch.cuda.set_device(local_rank)
+    cache = os.environ.get("EDUS_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "edus_bench_tmd22"))
+    if world > 1:
+        # one rank writes the model; the others wait for it
+        if rank == 0:
+            inp = workload_input(cache)
+        torch.distributed.barrier()
+        if rank != 0:
+            inp = workload_input(cache)
+    else:
+        inp = workload_input(cache)
+    cfg = pkg.model.parse_input(inp)
+    cfg.solver = pkg.edus.SOLVER_RK
+    cfg.order = 4
+    model = pkg.model.Model(cfg)
+    B = args.batch
+    s = model.solver(batch=B, device=local_rank)
+    # start inside the pulse, as in the middle of a production run
+    t_start = cfg.lasers[0].t0 - 2.0 * cfg.lasers[0].fwhm
+    s.time = t_start
+    stream = torch.cuda.ExternalStream(s.stream)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        s.step(1)
+    s.synchronize()
+    K = args.steps
+    launches0 = s.kernel_launches
+    # ---- device-timed region (inputs resident in HBM) ----
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        ev0.record(stream)
+        s.step(K)
+        ev1.record(stream)
+        s.synchronize()
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = s.kernel_launches - launches0
+    t_all = torch.tensor([ms], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t_all, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t_all.item())
+    value = B * K * world / (ms_max / 1e3)
+    clk = clocks.summary()
+
+    # ---- per-kernel event timing (roofline) over K more steps ----
+    s.set_profiling(True)
+    s.step(K)
+    plane_ms, plane_n = s.profile(0)
+    comm_ms, comm_n = s.profile(1)
+    s.set_profiling(False)
+    P, Nk = model.nb ** 2, model.Nk
+    pol = np.asarray(cfg.lasers[0].pol, dtype=float)
+    d_E = int(np.count_nonzero(pol))
+    plane_B, comm_B = algorithmic_bytes(P, Nk, B, d_E, cfg.coulomb)
+    plane_avg = plane_ms / max(plane_n, 1)
+    comm_avg = comm_ms / max(comm_n, 1)
+    peak, peak_kind = measured_peaks()
+    dominant = "plane_rhs_kernel" if plane_ms >= comm_ms else "commutator_kernel"
+    if dominant == "plane_rhs_kernel":
+        ach = plane_B / 4 / (plane_avg / 1e3) / 1e9
+    else:
+        ach = comm_B / 4 / (comm_avg / 1e3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        with open(tf) as f:
+            traffic = json.load(f).get(dominant)
+
+    # ---- end to end through the public API with host buffers ----
+    host_rho = torch.empty((model.Nk, model.nb, model.nb), dtype=torch.complex128).pin_memory()
+    host_rho.numpy()[:] = model.rho0k
+    out_rho = torch.empty_like(host_rho).pin_memory()
+    s.time = t_start
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ev_wall0 = time.perf_counter()
+    e0.record(stream)
+    for b in range(B):
+        s.set_state(host_rho.numpy(), b)
+    pops = []
+    for _ in range(K):
+        s.step(1)  # uploads the step's field table from pinned host memory
+        pops.append(s.population_wannier(0))  # device->host read of the step's result
+    for b in range(B):
+        s.get_state(b, out=out_rho.numpy())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_wall = time.perf_counter() - ev_wall0
+    e2e_ms = e0.elapsed_time(e1)
+    t_e2e = torch.tensor([max(e2e_ms, e2e_wall * 1e3)], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t_e2e, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = B * K * world / (float(t_e2e.item()) / 1e3)
+    S_bytes = model.Nk * model.nb ** 2 * 16
+    h2d = (B * S_bytes) / K + 4 * 48 * B
+    d2h = (B * S_bytes) / K + 8 * model.nb
+    finite = bool(np.isfinite(out_rho.numpy()).all())
+
+    result = {
+        "metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / K, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "form": "plain FP64 (drop-in), full nb^2 planes",
+        "config": {"workload": f"{WORKLOAD}: 22-orbital TMD-like, 72x72x1 k grid, HSEX (RK r0=40 A, eps=1), "
+                               f"RK4 dt=0.005 fs, batch={B} solve(s) per GPU",
+                   "batch": B, "l2": f"inputs larger than L2 (state {S_bytes / 1e6:.1f} MB x {B}; "
+                                     f"per-step working set {(plane_B + comm_B) / 1e9:.2f} GB)",
+                   "parallelism": f"replicas x{world}"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(ach, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": traffic,
+                     "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+                     "plane_kernel_ms": round(plane_avg, 5), "commutator_kernel_ms": round(comm_avg, 5),
+                     "plane_bytes_per_launch": plane_B / 4, "commutator_bytes_per_launch": comm_B / 4,
+                     "step_bytes": plane_B + comm_B,
+                     "step_GBps": round((plane_B + comm_B) / (ms_max / K / 1e3) / 1e9, 1)},
+        "e2e": {"value": round(e2e_value, 3), "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "finite": finite},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(inp, steps=args.cpu_steps)
+    s.close()
+    return result
+
+
+def cpu_baseline(inp, steps=2, threads=None):
+    """The FP64 CPU restatement (oracle/) timed on the host cores on a bounded
+    sample: `steps` RK4 steps of the same workload inside the pulse."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    threads = threads or os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    cfg = pyoracle.load_input(inp)
+    cfg.solver, cfg.order = 1, 4
+    o = pyoracle.Oracle(cfg)
+    o.time = cfg.lasers[0].t0 - 2.0 * cfg.lasers[0].fwhm
+    o.step(1)  # warm-up (page-in, thread pool)
+    t = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t
+    return {"value": round(steps / dt, 5), "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} RK4 steps of the full {WORKLOAD} workload (72x72, nb=22, HSEX), "
+                      f"{dt:.1f} s, OpenMP {threads} threads"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU propagation on the host cores."""
+    cache = os.environ.get("EDUS_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "edus_bench_tmd22"))
+    inp = workload_input(cache)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    threads = os.cpu_count()
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    cfg = pyoracle.load_input(inp)
+    cfg.solver, cfg.order = 1, 4
+    o = pyoracle.Oracle(cfg)
+    o.time = cfg.lasers[0].t0 - 2.0 * cfg.lasers[0].fwhm
+    K = max(1, min(args.steps, args.ref_max_steps))
+    W = min(args.warmup, 1)
+    o.step(W)
+    t = time.perf_counter()
+    o.step(K)
+    dt = time.perf_counter() - t
+    v = K / dt
+    return {
+        "metric": METRIC, "impl": "reference", "value": round(v, 5), "unit": "steps/s", "n_gpus": 0,
+        "steps": K, "warmup": W, "ms_per_step": round(dt / K * 1e3, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{WORKLOAD}: 22-orbital TMD-like, 72x72x1 k grid, HSEX, RK4 dt=0.005 fs",
+                   "parallelism": "host cores"},
+        "cpu_baseline": {"value": round(v, 5), "unit": "steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{K} RK4 steps (after {W} warm-up) of the full workload; the reference "
+                                   f"itself needs MKL/FFTW/MPI, absent here, so its FP64 restatement runs"},
+        "e2e": {"value": round(v, 5), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=1)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--ref-max-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    res = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        import torch
+
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,730 @@
+// Host side of the C ABI declared in include/edus_gpu.h.
+//
+// One handle = one model (H0, xi, W, rho0, Hartree) shared by `batch`
+// independent solves, each with its own lasers and density matrix.  All
+// device memory is allocated in edus_create / edus_upload_model; the step
+// loop allocates nothing.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include <stdexcept>
+#include "../../include/edus_gpu.h"
+#include "kernels.cuh"
+
+using namespace edus;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct edus_handle {
+    edus_desc d{};
+    int N[3] = {1, 1, 1};
+    int Nk = 0, nb = 0, P = 0, B = 1;
+    size_t S = 0;  // complex numbers per solve (P*Nk)
+    cudaStream_t stream = nullptr;
+    std::string err;
+    bool model_ready = false;
+    double t = 0.0;
+    double A[9] = {0};  // lattice, row-major, vectors in columns
+    PlanePlan plan{};
+    int smem_plane = 0, smem_comm = 0, TK = 4;
+    unsigned long long launches = 0;
+    size_t dev_bytes = 0;
+    std::vector<std::vector<edus_laser>> lasers;
+    // AB ring (DESolver.hpp:47, rotated after each step)
+    int index[5] = {0, 1, 2, 3, 4};
+    double beta[5] = {0, 0, 0, 0, 0};
+    // device buffers
+    double2 *H0 = nullptr, *xi[3] = {nullptr, nullptr, nullptr};
+    double2* rho0p = nullptr;
+    double* Wp = nullptr;
+    double2 *hartree = nullptr, *rho0diag = nullptr;
+    double2 *y = nullptr, *aux = nullptr, *acc = nullptr, *hist[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double2 *G = nullptr, *Hee = nullptr, *diag0 = nullptr;
+    double2* roots = nullptr;
+    double* rpos = nullptr;
+    StageField* field = nullptr;   // device table [chunk][stage][B]
+    StageField* field_host[2] = {nullptr, nullptr};  // pinned
+    cudaEvent_t field_ev[2] = {nullptr, nullptr};
+    int field_cur = 0;
+    int chunk = 256;
+    double2* stage = nullptr;      // [Nk][P] staging for transposes
+    double2* tmp_in = nullptr;     // edus_rhs input/output in plane layout
+    double2* tmp_out = nullptr;
+    double* popbuf = nullptr;
+    int* flag = nullptr;
+    std::vector<void*> allocs;
+    // profiling: event pairs per launch, resolved in edus_get_profile
+    bool profiling = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+    double prof_ms[2] = {0, 0};
+    unsigned long long prof_n[2] = {0, 0};
+};
+
+namespace {
+
+int fail(edus_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define CU(h, expr)                                                                              \
+    do {                                                                                         \
+        cudaError_t e_ = (expr);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail(h, EDUS_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int dalloc(edus_handle* h, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(h, EDUS_ERR_NOMEM, std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    }
+    h->allocs.push_back(*p);
+    h->dev_bytes += bytes;
+    return EDUS_OK;
+}
+
+#define ALLOC(h, ptr, bytes)                                      \
+    do {                                                          \
+        int rc_ = dalloc(h, (void**)&(ptr), (size_t)(bytes));     \
+        if (rc_ != EDUS_OK) return rc_;                           \
+    } while (0)
+
+// Radices of one axis in DIF order: powers of two first (8, then 4/2), odd
+// radices last (they sit at the short strides, where odd spacing avoids
+// shared-memory bank conflicts).
+bool factor_axis(int n, std::vector<int>& r) {
+    r.clear();
+    int m = n;
+    while (m % 8 == 0) { r.push_back(8); m /= 8; }
+    if (m % 4 == 0) { r.push_back(4); m /= 4; }
+    if (m % 2 == 0) { r.push_back(2); m /= 2; }
+    for (int q : {3, 5, 7})
+        while (m % q == 0) { r.push_back(q); m /= q; }
+    return m == 1 && (int)r.size() <= kMaxStages;
+}
+
+// frequency index stored at each position after the DIF pass
+void dif_positions(int n, const std::vector<int>& r, std::vector<int>& freq_at_pos) {
+    freq_at_pos.assign(n, 0);
+    for (int k = 0; k < n; ++k) {
+        int pos = 0, len = n, kk = k;
+        for (int radix : r) {
+            len /= radix;
+            pos += (kk % radix) * len;
+            kk /= radix;
+        }
+        freq_at_pos[pos] = k;
+    }
+}
+
+void field_at(const std::vector<edus_laser>& ls, const double A[9], double t, StageField& f) {
+    // SetOfLaser::operator() (Laser.hpp:143-150) with Laser::operator()
+    // (Laser.cpp:131-134), envelope (Laser.cpp:96-104), carrier (Laser.cpp:35-38)
+    const double pi = 3.14159265358979323846;
+    double E[3] = {0, 0, 0};
+    for (const auto& L : ls) {
+        double nrm = std::sqrt(L.pol[0] * L.pol[0] + L.pol[1] * L.pol[1] + L.pol[2] * L.pol[2]);
+        double pol[3] = {L.pol[0] / nrm, L.pol[1] / nrm, L.pol[2] / nrm};
+        // Laser::set_Polarization normalises a second time (Laser.cpp:197-200)
+        double n2 = std::sqrt(pol[0] * pol[0] + pol[1] * pol[1] + pol[2] * pol[2]);
+        for (int d = 0; d < 3; ++d) pol[d] = pol[d] / n2;
+        double a;
+        const double amp = std::sqrt(L.intensity);
+        if (L.envelope == EDUS_ENVELOPE_SIN2) {
+            const double period = 2. * pi / L.omega;
+            const double duration = L.cycles * period;
+            const double tt = t - L.t0;
+            const double env = (tt <= 1.e-07 || tt > duration) ? 0. : std::pow(std::sin(pi * tt / duration), 2.);
+            a = amp * env * std::sin(L.omega * (t - L.t0) + L.phase);
+        } else {
+            const double tt = t - L.t0;
+            const double env = std::exp(-2.0 * std::log(2.0) * tt * tt / (L.fwhm * L.fwhm));
+            a = amp * env * std::cos(L.omega * tt + L.phase);
+        }
+        for (int d = 0; d < 3; ++d) E[d] += a * pol[d];
+    }
+    for (int d = 0; d < 3; ++d) f.E[d] = E[d];
+    for (int c = 0; c < 3; ++c) f.g[c] = A[0 * 3 + c] * E[0] + A[1 * 3 + c] * E[1] + A[2 * 3 + c] * E[2];
+}
+
+int choose_tk(int P) {
+    int tk = 1;
+    while (tk * P < 1024 && tk < 64) tk *= 2;
+    if (tk < 4) tk = 4;
+    // keep the two smem tiles within 64 KB where possible
+    while (tk > 4 && (size_t)2 * P * tk * 16 > 64 * 1024) tk /= 2;
+    return tk;
+}
+
+cudaEvent_t prof_event(edus_handle* h) {
+    if (!h->prof_pool.empty()) {
+        cudaEvent_t e = h->prof_pool.back();
+        h->prof_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void prof_begin(edus_handle* h, cudaEvent_t* e0) {
+    *e0 = nullptr;
+    if (!h->profiling) return;
+    *e0 = prof_event(h);
+    cudaEventRecord(*e0, h->stream);
+}
+
+void prof_end(edus_handle* h, int kind, cudaEvent_t e0) {
+    if (!h->profiling || !e0) return;
+    cudaEvent_t e1 = prof_event(h);
+    cudaEventRecord(e1, h->stream);
+    h->prof_pending.push_back({kind, {e0, e1}});
+}
+
+void prof_resolve(edus_handle* h) {
+    for (auto& pe : h->prof_pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, pe.second.first, pe.second.second) == cudaSuccess) {
+            h->prof_ms[pe.first] += ms;
+            h->prof_n[pe.first] += 1;
+        }
+        h->prof_pool.push_back(pe.second.first);
+        h->prof_pool.push_back(pe.second.second);
+    }
+    h->prof_pending.clear();
+}
+
+int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double2* G, double2* Hee,
+                 long long out_bstride, const StageField* field, int nbatch) {
+    dim3 grid(h->P, nbatch);
+    cudaEvent_t e0;
+    prof_begin(h, &e0);
+    if (h->d.coulomb)
+        plane_rhs_kernel<true><<<grid, 512, h->smem_plane, h->stream>>>(in, in_bstride, G, Hee, out_bstride, h->rho0p,
+                                                                         h->Wp, h->diag0, field, h->roots, h->rpos,
+                                                                         h->plan, h->nb, 1.0 / h->Nk);
+    else
+        plane_rhs_kernel<false><<<grid, 512, h->smem_plane, h->stream>>>(in, in_bstride, G, Hee, out_bstride, h->rho0p,
+                                                                          h->Wp, h->diag0, field, h->roots, h->rpos,
+                                                                          h->plan, h->nb, 1.0 / h->Nk);
+    h->launches++;
+    CU(h, cudaGetLastError());
+    prof_end(h, 0, e0);
+    return EDUS_OK;
+}
+
+template <int MODE>
+int launch_comm_mode(edus_handle* h, const StageArgs& a, int nbatch) {
+    dim3 grid((h->Nk + h->TK - 1) / h->TK, nbatch);
+    cudaEvent_t e0;
+    prof_begin(h, &e0);
+    if (h->d.coulomb)
+        commutator_kernel<MODE, true><<<grid, 256, h->smem_comm, h->stream>>>(a);
+    else
+        commutator_kernel<MODE, false><<<grid, 256, h->smem_comm, h->stream>>>(a);
+    h->launches++;
+    CU(h, cudaGetLastError());
+    prof_end(h, 1, e0);
+    return EDUS_OK;
+}
+
+int launch_comm(edus_handle* h, int mode, const StageArgs& a, int nbatch) {
+    switch (mode) {
+        case MODE_RHS: return launch_comm_mode<MODE_RHS>(h, a, nbatch);
+        case MODE_RK1: return launch_comm_mode<MODE_RK1>(h, a, nbatch);
+        case MODE_RK2: return launch_comm_mode<MODE_RK2>(h, a, nbatch);
+        case MODE_RK3: return launch_comm_mode<MODE_RK3>(h, a, nbatch);
+        case MODE_RK4: return launch_comm_mode<MODE_RK4>(h, a, nbatch);
+        case MODE_AB: return launch_comm_mode<MODE_AB>(h, a, nbatch);
+    }
+    return fail(h, EDUS_ERR_ARG, "bad stage mode");
+}
+
+template <typename K>
+int set_smem(edus_handle* h, K kernel, int bytes) {
+    CU(h, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    return EDUS_OK;
+}
+
+StageArgs base_args(edus_handle* h) {
+    StageArgs a{};
+    a.H0 = h->H0;
+    for (int d = 0; d < 3; ++d) a.xi[d] = h->xi[d];
+    a.Hee = h->Hee;
+    a.G = h->G;
+    a.hartree = h->hartree;
+    a.rho0diag = h->rho0diag;
+    a.diag0 = h->diag0;
+    a.bstride = (long long)h->S;
+    a.Nk = h->Nk;
+    a.nb = h->nb;
+    a.TK = h->TK;
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* edus_last_error(const edus_handle* h) {
+    if (!h) return g_create_error.c_str();
+    return h->err.c_str();
+}
+
+int edus_create(const edus_desc* desc, edus_handle** out) {
+    if (!desc || !out) return fail(nullptr, EDUS_ERR_ARG, "edus_create: NULL argument");
+    *out = nullptr;
+    const edus_desc& d = *desc;
+    for (int i = 0; i < 3; ++i)
+        if (d.grid[i] < 1) return fail(nullptr, EDUS_ERR_ARG, "grid dimensions must be >= 1");
+    if (d.nbands < 1 || d.nbands > 64) return fail(nullptr, EDUS_ERR_ARG, "nbands must be in [1, 64]");
+    if (d.solver != EDUS_SOLVER_RK && d.solver != EDUS_SOLVER_AB) return fail(nullptr, EDUS_ERR_ARG, "unknown solver");
+    if (d.solver == EDUS_SOLVER_RK && d.order != 4)
+        return fail(nullptr, EDUS_ERR_UNSUPPORTED, "RK is implemented for order 4 only (DESolver.hpp:157)");
+    if (d.solver == EDUS_SOLVER_AB && d.order != 4 && d.order != 5)
+        return fail(nullptr, EDUS_ERR_UNSUPPORTED, "order not implemented for AB (DESolver.hpp:120-124)");
+    if (d.precision != EDUS_PREC_FP64) return fail(nullptr, EDUS_ERR_UNSUPPORTED, "precision not supported");
+    if (d.batch < 1) return fail(nullptr, EDUS_ERR_ARG, "batch must be >= 1");
+    if (!(d.dt > 0.0) || !std::isfinite(d.dt)) return fail(nullptr, EDUS_ERR_ARG, "dt must be positive and finite");
+
+    edus_handle* h = new edus_handle();
+    h->d = d;
+    for (int i = 0; i < 3; ++i) h->N[i] = d.grid[i];
+    h->Nk = d.grid[0] * d.grid[1] * d.grid[2];
+    h->nb = d.nbands;
+    h->P = d.nbands * d.nbands;
+    h->B = d.batch;
+    h->S = (size_t)h->P * h->Nk;
+    h->lasers.assign(h->B, {});
+    auto bail = [&](int rc) {
+        std::string m = h->err;
+        edus_destroy(h);
+        g_create_error = m;
+        return rc;
+    };
+    if (cudaSetDevice(d.device) != cudaSuccess) return bail(fail(h, EDUS_ERR_CUDA, "cudaSetDevice failed"));
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(h, EDUS_ERR_CUDA, "cudaStreamCreate failed"));
+
+    // FFT plan per axis
+    std::vector<double2> roots;
+    std::vector<double> rpos;
+    int stride = 1;
+    for (int ax = 2; ax >= 0; --ax) {
+        AxisPlan& A = h->plan.ax[ax];
+        A.n = h->N[ax];
+        A.inner = stride;
+        stride *= A.n;
+        std::vector<int> r;
+        if (!factor_axis(A.n, r))
+            return bail(fail(h, EDUS_ERR_UNSUPPORTED, "grid size " + std::to_string(A.n) +
+                                                          " has a prime factor other than 2, 3, 5, 7"));
+        A.nst = (int)r.size();
+        int L = A.n;
+        for (int s = 0; s < A.nst; ++s) {
+            A.r[s] = r[s];
+            L /= r[s];
+            A.L[s] = L;
+        }
+        A.rootoff = (int)roots.size();
+        for (int j = 0; j < A.n; ++j) {
+            long double a = -2.0L * 3.14159265358979323846264338327950288L * j / A.n;
+            roots.push_back(make_double2((double)cosl(a), (double)sinl(a)));
+        }
+        A.rposoff = (int)rpos.size();
+        std::vector<int> fp;
+        dif_positions(A.n, r, fp);
+        for (int q = 0; q < A.n; ++q) {
+            int j = fp[q];
+            // Gamma-centred coordinate, MeshGrid.cpp:352-375 with [-N/2, N/2)
+            rpos.push_back(2 * j >= A.n ? double(j - A.n) : double(j));
+        }
+    }
+    h->plan.Nk = h->Nk;
+
+    int dev_smem = 0;
+    cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, d.device);
+    const size_t plane_bytes = (size_t)h->Nk * sizeof(double2) * (d.coulomb ? 2 : 1);
+    if (plane_bytes > (size_t)dev_smem)
+        return bail(fail(h, EDUS_ERR_UNSUPPORTED,
+                         "k grid of " + std::to_string(h->Nk) + " points does not fit one plane" +
+                             (d.coulomb ? " pair" : "") + " in shared memory (" + std::to_string(dev_smem) + " B)"));
+    h->smem_plane = (int)plane_bytes;
+    h->TK = choose_tk(h->P);
+    h->smem_comm = (int)((2 * (size_t)h->P * h->TK + h->nb) * sizeof(double2));
+    if (h->smem_comm > dev_smem) return bail(fail(h, EDUS_ERR_UNSUPPORTED, "too many bands for the commutator tile"));
+    int rc;
+    if ((rc = set_smem(h, plane_rhs_kernel<true>, h->smem_plane))) return bail(rc);
+    if ((rc = set_smem(h, plane_rhs_kernel<false>, h->smem_plane))) return bail(rc);
+#define SETC(M)                                                                                   \
+    if ((rc = set_smem(h, commutator_kernel<M, true>, h->smem_comm))) return bail(rc);           \
+    if ((rc = set_smem(h, commutator_kernel<M, false>, h->smem_comm))) return bail(rc);
+    SETC(MODE_RHS) SETC(MODE_RK1) SETC(MODE_RK2) SETC(MODE_RK3) SETC(MODE_RK4) SETC(MODE_AB)
+#undef SETC
+
+    const size_t Sb = h->S * sizeof(double2);
+    const size_t SBb = Sb * h->B;
+#define TRY_ALLOC(ptr, bytes) \
+    if ((rc = dalloc(h, (void**)&(ptr), (bytes)))) return bail(rc);
+    TRY_ALLOC(h->H0, Sb);
+    for (int i = 0; i < 3; ++i) TRY_ALLOC(h->xi[i], Sb);
+    TRY_ALLOC(h->y, SBb);
+    TRY_ALLOC(h->G, SBb);
+    TRY_ALLOC(h->stage, Sb);
+    if (d.solver == EDUS_SOLVER_RK) {
+        TRY_ALLOC(h->aux, SBb);
+        TRY_ALLOC(h->acc, SBb);
+    } else {
+        for (int i = 0; i < d.order; ++i) {
+            TRY_ALLOC(h->hist[i], SBb);
+            // zero history (DESolver.cpp:26-29, mdContainers_definitions.hpp:91)
+            if (cudaMemsetAsync(h->hist[i], 0, SBb, h->stream) != cudaSuccess)
+                return bail(fail(h, EDUS_ERR_CUDA, "cudaMemsetAsync failed"));
+        }
+        if (d.order == 4) {
+            const double b[5] = {55. / 24., -59. / 24., 37. / 24., -3. / 8., 0.};
+            std::copy(b, b + 5, h->beta);
+        } else {
+            const double b[5] = {1901. / 720., -2774. / 720., 2616. / 720., -1274. / 720., 251. / 720.};
+            std::copy(b, b + 5, h->beta);
+        }
+    }
+    if (d.coulomb) {
+        TRY_ALLOC(h->Hee, SBb);
+        TRY_ALLOC(h->rho0p, Sb);
+        TRY_ALLOC(h->Wp, (size_t)h->S * sizeof(double));
+        TRY_ALLOC(h->hartree, h->P * sizeof(double2));
+        TRY_ALLOC(h->rho0diag, h->nb * sizeof(double2));
+        TRY_ALLOC(h->diag0, (size_t)h->B * h->nb * sizeof(double2));
+    }
+    TRY_ALLOC(h->roots, roots.size() * sizeof(double2));
+    TRY_ALLOC(h->rpos, rpos.size() * sizeof(double));
+    TRY_ALLOC(h->field, (size_t)h->chunk * 4 * h->B * sizeof(StageField));
+    TRY_ALLOC(h->popbuf, h->nb * sizeof(double));
+    TRY_ALLOC(h->flag, sizeof(int));
+#undef TRY_ALLOC
+    for (int i = 0; i < 2; ++i) {
+        if (cudaMallocHost((void**)&h->field_host[i], (size_t)h->chunk * 4 * h->B * sizeof(StageField)) != cudaSuccess)
+            return bail(fail(h, EDUS_ERR_NOMEM, "cudaMallocHost failed"));
+        if (cudaEventCreateWithFlags(&h->field_ev[i], cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(h, EDUS_ERR_CUDA, "cudaEventCreate failed"));
+        cudaEventRecord(h->field_ev[i], h->stream);
+    }
+    if (cudaMemcpyAsync(h->roots, roots.data(), roots.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaMemcpyAsync(h->rpos, rpos.data(), rpos.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->y, 0, SBb, h->stream) != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess)
+        return bail(fail(h, EDUS_ERR_CUDA, "initial upload failed"));
+    *out = h;
+    return EDUS_OK;
+}
+
+int edus_destroy(edus_handle* h) {
+    if (!h) return EDUS_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    prof_resolve(h);
+    for (cudaEvent_t e : h->prof_pool) cudaEventDestroy(e);
+    for (void* p : h->allocs) cudaFree(p);
+    for (int i = 0; i < 2; ++i) {
+        if (h->field_host[i]) cudaFreeHost(h->field_host[i]);
+        if (h->field_ev[i]) cudaEventDestroy(h->field_ev[i]);
+    }
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return EDUS_OK;
+}
+
+int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, const double* lattice,
+                      const double* W_R, const double* rho0_R, const double* hartree) {
+    if (!h) return EDUS_ERR_ARG;
+    if (!H0_k || !xi_k || !lattice) return fail(h, EDUS_ERR_ARG, "H0_k, xi_k and lattice are required");
+    if (h->d.coulomb && (!W_R || !rho0_R || !hartree))
+        return fail(h, EDUS_ERR_ARG, "coulomb=1 needs W_R, rho0_R and hartree");
+    CU(h, cudaSetDevice(h->d.device));
+    std::memcpy(h->A, lattice, sizeof(h->A));
+    const int Nk = h->Nk, P = h->P;
+    const size_t Sb = h->S * sizeof(double2);
+    dim3 tb(32, 8);
+    dim3 tg((Nk + 31) / 32, (P + 31) / 32);
+    auto up = [&](const double* src, double2* dst) -> int {
+        CU(h, cudaMemcpyAsync(h->stage, src, Sb, cudaMemcpyHostToDevice, h->stream));
+        transpose_kp_to_pk<<<tg, tb, 0, h->stream>>>(h->stage, dst, Nk, P);
+        h->launches++;
+        CU(h, cudaGetLastError());
+        return EDUS_OK;
+    };
+    int rc;
+    if ((rc = up(H0_k, h->H0))) return rc;
+    for (int d = 0; d < 3; ++d)
+        if ((rc = up(xi_k + 2 * h->S * d, h->xi[d]))) return rc;
+    if (h->d.coulomb) {
+        // R-space arrays go to the digit-reversed positions of the plane FFT
+        std::vector<int> fq[3];
+        for (int ax = 0; ax < 3; ++ax) {
+            std::vector<int> r;
+            for (int s = 0; s < h->plan.ax[ax].nst; ++s) r.push_back(h->plan.ax[ax].r[s]);
+            dif_positions(h->N[ax], r, fq[ax]);
+        }
+        std::vector<double> w(h->S);
+        std::vector<double2> r0(h->S);
+        const int N1 = h->N[1], N2 = h->N[2];
+        for (int q0 = 0; q0 < h->N[0]; ++q0)
+            for (int q1 = 0; q1 < N1; ++q1)
+                for (int q2 = 0; q2 < N2; ++q2) {
+                    const int pos = (q0 * N1 + q1) * N2 + q2;
+                    const int iR = (fq[0][q0] * N1 + fq[1][q1]) * N2 + fq[2][q2];
+                    for (int p = 0; p < P; ++p) {
+                        const double* wsrc = W_R + 2 * ((size_t)iR * P + p);
+                        if (wsrc[1] != 0.0)
+                            return fail(h, EDUS_ERR_ARG, "W_R must be real (the screened potential has no imaginary part)");
+                        w[(size_t)p * Nk + pos] = wsrc[0];
+                        const double* rsrc = rho0_R + 2 * ((size_t)iR * P + p);
+                        r0[(size_t)p * Nk + pos] = make_double2(rsrc[0], rsrc[1]);
+                    }
+                }
+        std::vector<double2> d0(h->nb);
+        for (int n = 0; n < h->nb; ++n) d0[n] = make_double2(rho0_R[2 * (n * h->nb + n)], rho0_R[2 * (n * h->nb + n) + 1]);
+        CU(h, cudaMemcpyAsync(h->Wp, w.data(), h->S * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CU(h, cudaMemcpyAsync(h->rho0p, r0.data(), Sb, cudaMemcpyHostToDevice, h->stream));
+        CU(h, cudaMemcpyAsync(h->hartree, hartree, P * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+        CU(h, cudaMemcpyAsync(h->rho0diag, d0.data(), h->nb * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+        CU(h, cudaStreamSynchronize(h->stream));  // host vectors go out of scope
+    }
+    CU(h, cudaStreamSynchronize(h->stream));
+    h->model_ready = true;
+    return EDUS_OK;
+}
+
+int edus_set_lasers(edus_handle* h, int b, int n, const edus_laser* lasers) {
+    if (!h) return EDUS_ERR_ARG;
+    if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
+    if (n < 0 || (n > 0 && !lasers)) return fail(h, EDUS_ERR_ARG, "bad laser list");
+    std::vector<edus_laser> v(lasers, lasers + n);
+    for (auto& L : v) {
+        const double nrm = std::sqrt(L.pol[0] * L.pol[0] + L.pol[1] * L.pol[1] + L.pol[2] * L.pol[2]);
+        if (!(nrm > 0)) return fail(h, EDUS_ERR_ARG, "laser polarisation must be non-zero");
+        if (L.envelope == EDUS_ENVELOPE_SIN2 && !(L.omega != 0)) return fail(h, EDUS_ERR_ARG, "sin2 laser needs omega != 0");
+        if (L.envelope == EDUS_ENVELOPE_GAUSS && !(L.fwhm > 0)) return fail(h, EDUS_ERR_ARG, "gaussian laser needs fwhm > 0");
+        if (L.envelope != EDUS_ENVELOPE_SIN2 && L.envelope != EDUS_ENVELOPE_GAUSS)
+            return fail(h, EDUS_ERR_ARG, "unknown envelope");
+    }
+    h->lasers[b] = v;
+    return EDUS_OK;
+}
+
+int edus_set_state(edus_handle* h, int b, const double* rho_k) {
+    if (!h || !rho_k) return EDUS_ERR_ARG;
+    if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
+    CU(h, cudaSetDevice(h->d.device));
+    dim3 tb(32, 8), tg((h->Nk + 31) / 32, (h->P + 31) / 32);
+    CU(h, cudaMemcpyAsync(h->stage, rho_k, h->S * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    transpose_kp_to_pk<<<tg, tb, 0, h->stream>>>(h->stage, h->y + (size_t)b * h->S, h->Nk, h->P);
+    h->launches++;
+    CU(h, cudaGetLastError());
+    CU(h, cudaStreamSynchronize(h->stream));
+    return EDUS_OK;
+}
+
+int edus_get_state(edus_handle* h, int b, double* rho_k) {
+    if (!h || !rho_k) return EDUS_ERR_ARG;
+    if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
+    CU(h, cudaSetDevice(h->d.device));
+    dim3 tb(32, 8), tg((h->P + 31) / 32, (h->Nk + 31) / 32);
+    transpose_pk_to_kp<<<tg, tb, 0, h->stream>>>(h->y + (size_t)b * h->S, h->stage, h->Nk, h->P);
+    h->launches++;
+    CU(h, cudaGetLastError());
+    CU(h, cudaMemcpyAsync(rho_k, h->stage, h->S * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    return EDUS_OK;
+}
+
+int edus_set_time(edus_handle* h, double t) {
+    if (!h) return EDUS_ERR_ARG;
+    h->t = t;
+    return EDUS_OK;
+}
+
+int edus_get_time(const edus_handle* h, double* t) {
+    if (!h || !t) return EDUS_ERR_ARG;
+    *t = h->t;
+    return EDUS_OK;
+}
+
+int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k) {
+    if (!h || !in_k || !out_k) return EDUS_ERR_ARG;
+    if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "edus_upload_model must be called first");
+    CU(h, cudaSetDevice(h->d.device));
+    int rc;
+    if (!h->tmp_in) {
+        if ((rc = dalloc(h, (void**)&h->tmp_in, h->S * sizeof(double2)))) return rc;
+        if ((rc = dalloc(h, (void**)&h->tmp_out, h->S * sizeof(double2)))) return rc;
+    }
+    // field of solve 0 at time t, in slot 0 of the table (wait for the
+    // previous user of the pinned buffer)
+    CU(h, cudaEventSynchronize(h->field_ev[0]));
+    field_at(h->lasers[0], h->A, t, h->field_host[0][0]);
+    CU(h, cudaMemcpyAsync(h->field, h->field_host[0], sizeof(StageField), cudaMemcpyHostToDevice, h->stream));
+    CU(h, cudaEventRecord(h->field_ev[0], h->stream));
+    dim3 tb(32, 8), tg((h->Nk + 31) / 32, (h->P + 31) / 32);
+    CU(h, cudaMemcpyAsync(h->stage, in_k, h->S * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    transpose_kp_to_pk<<<tg, tb, 0, h->stream>>>(h->stage, h->tmp_in, h->Nk, h->P);
+    h->launches++;
+    if ((rc = launch_plane(h, h->tmp_in, 0, h->G, h->Hee, 0, h->field, 1))) return rc;
+    StageArgs a = base_args(h);
+    a.rho = h->tmp_in;
+    a.field = h->field;
+    a.out = h->tmp_out;
+    if ((rc = launch_comm(h, MODE_RHS, a, 1))) return rc;
+    dim3 tg2((h->P + 31) / 32, (h->Nk + 31) / 32);
+    transpose_pk_to_kp<<<tg2, tb, 0, h->stream>>>(h->tmp_out, h->stage, h->Nk, h->P);
+    h->launches++;
+    CU(h, cudaGetLastError());
+    CU(h, cudaMemcpyAsync(out_k, h->stage, h->S * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    return EDUS_OK;
+}
+
+int edus_step(edus_handle* h, int n) {
+    if (!h || n < 0) return EDUS_ERR_ARG;
+    if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "edus_upload_model must be called first");
+    CU(h, cudaSetDevice(h->d.device));
+    const bool rk = h->d.solver == EDUS_SOLVER_RK;
+    const int nst = rk ? 4 : 1;
+    const double dt = h->d.dt;
+    const int B = h->B;
+    const long long bs = (long long)h->S;
+    int rc;
+    for (int s0 = 0; s0 < n; s0 += h->chunk) {
+        const int cnt = std::min(h->chunk, n - s0);
+        // host field table for this chunk: stage times as DESolver uses them,
+        // with CurrentTime accumulated by += dt (DESolver.hpp:167-186, 205-219)
+        const int buf = h->field_cur;
+        h->field_cur ^= 1;
+        CU(h, cudaEventSynchronize(h->field_ev[buf]));
+        StageField* tab = h->field_host[buf];
+        double t = h->t;
+        for (int i = 0; i < cnt; ++i) {
+            double ts[4] = {t, t + dt / 2., t + dt / 2., t + dt};
+            for (int s = 0; s < nst; ++s)
+                for (int b = 0; b < B; ++b) field_at(h->lasers[b], h->A, ts[s], tab[((size_t)i * nst + s) * B + b]);
+            t += dt;
+        }
+        // the device table of the previous chunk is no longer read once the
+        // kernels before this copy (same stream) have run
+        CU(h, cudaMemcpyAsync(h->field, tab, (size_t)cnt * nst * B * sizeof(StageField), cudaMemcpyHostToDevice, h->stream));
+        CU(h, cudaEventRecord(h->field_ev[buf], h->stream));
+        for (int i = 0; i < cnt; ++i) {
+            const StageField* fs = h->field + (size_t)i * nst * B;
+            StageArgs a = base_args(h);
+            a.y = h->y;
+            if (rk) {
+                a.aux = h->aux;
+                a.acc = h->acc;
+                const double c0[4] = {dt / 2., dt / 2., dt, dt / 6.};
+                const double c1[4] = {dt / 6., dt / 3., dt / 3., 0.};
+                for (int s = 0; s < 4; ++s) {
+                    const double2* in = (s == 0) ? h->y : h->aux;
+                    if ((rc = launch_plane(h, in, bs, h->G, h->Hee, bs, fs + (size_t)s * B, B))) return rc;
+                    a.rho = in;
+                    a.field = fs + (size_t)s * B;
+                    a.c[0] = c0[s];
+                    a.c[1] = c1[s];
+                    if ((rc = launch_comm(h, MODE_RK1 + s, a, B))) return rc;
+                }
+            } else {
+                if ((rc = launch_plane(h, h->y, bs, h->G, h->Hee, bs, fs, B))) return rc;
+                a.rho = h->y;
+                a.field = fs;
+                a.order = h->d.order;
+                for (int q = 0; q < h->d.order; ++q) {
+                    a.hist[q] = h->hist[h->index[q]];
+                    a.c[q] = dt * h->beta[q];
+                }
+                if ((rc = launch_comm(h, MODE_AB, a, B))) return rc;
+                // rotate the ring (DESolver.hpp:212-217)
+                const int ord = h->d.order;
+                int tmp = h->index[ord - 1];
+                for (int q = ord - 1; q > 0; --q) h->index[q] = h->index[q - 1];
+                h->index[0] = tmp;
+            }
+            h->t += dt;
+        }
+    }
+    return EDUS_OK;
+}
+
+int edus_synchronize(edus_handle* h) {
+    if (!h) return EDUS_ERR_ARG;
+    CU(h, cudaSetDevice(h->d.device));
+    CU(h, cudaStreamSynchronize(h->stream));
+    return EDUS_OK;
+}
+
+int edus_population_wannier(edus_handle* h, int b, double* pop) {
+    if (!h || !pop) return EDUS_ERR_ARG;
+    if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
+    CU(h, cudaSetDevice(h->d.device));
+    population_kernel<<<h->nb, 256, 0, h->stream>>>(h->y + (size_t)b * h->S, h->Nk, h->nb, h->popbuf);
+    h->launches++;
+    CU(h, cudaGetLastError());
+    CU(h, cudaMemcpyAsync(pop, h->popbuf, h->nb * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    return EDUS_OK;
+}
+
+int edus_get_stream(const edus_handle* h, void** stream) {
+    if (!h || !stream) return EDUS_ERR_ARG;
+    *stream = (void*)h->stream;
+    return EDUS_OK;
+}
+
+int edus_set_profiling(edus_handle* h, int on) {
+    if (!h) return EDUS_ERR_ARG;
+    if (on && !h->profiling) {
+        CU(h, cudaStreamSynchronize(h->stream));
+        prof_resolve(h);
+        h->prof_ms[0] = h->prof_ms[1] = 0;
+        h->prof_n[0] = h->prof_n[1] = 0;
+    }
+    h->profiling = on != 0;
+    return EDUS_OK;
+}
+
+int edus_get_profile(edus_handle* h, int kind, double* total_ms, unsigned long long* launches) {
+    if (!h || kind < 0 || kind > 1 || !total_ms || !launches) return EDUS_ERR_ARG;
+    CU(h, cudaStreamSynchronize(h->stream));
+    prof_resolve(h);
+    *total_ms = h->prof_ms[kind];
+    *launches = h->prof_n[kind];
+    return EDUS_OK;
+}
+
+int edus_device_bytes(const edus_handle* h, unsigned long long* bytes) {
+    if (!h || !bytes) return EDUS_ERR_ARG;
+    *bytes = h->dev_bytes;
+    return EDUS_OK;
+}
+
+int edus_kernel_launches(const edus_handle* h, unsigned long long* n) {
+    if (!h || !n) return EDUS_ERR_ARG;
+    *n = h->launches;
+    return EDUS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,279 @@
+// Device kernels of one right-hand-side evaluation and of the time steppers.
+//
+// HBM layout (all device arrays): plane-major, [batch][p][k] with p = n*nb+m
+// the band pair and k the grid point, complex128 as double2.  A plane is one
+// band pair over the whole grid (Nk contiguous complex numbers), so
+//   * the plane kernel streams whole planes (one 16-byte vector per thread,
+//     fully coalesced) into shared memory for the k<->R transforms, and
+//   * the commutator kernel reads a tile of TK consecutive k of every plane:
+//     TK*16-byte contiguous segments.
+// R-space model arrays (W, rho0) are stored in the digit-reversed position
+// order that the in-place forward FFT leaves (see fft_plane.cuh).
+#pragma once
+#include <cuda_runtime.h>
+#include "fft_plane.cuh"
+
+namespace edus {
+
+// Field of one solve at one stage: E (Cartesian, a.u.) and g = A^T E, so that
+// R.E = g . R_crys for the Gamma-centred crystal coordinates R_crys.
+struct StageField {
+    double E[3];
+    double g[3];
+};
+
+// ---------------------------------------------------------------------------
+// Plane kernel: one CTA per (band pair p, solve b).
+//   rho_R  = FFT_{-1}(rho_k) / Nk                      (Operator::go_to_R)
+//   G_R    = i (R.E) rho_R                             (kGradient R branch)
+//   Hee_R  = -W (rho_R - rho0_R)                       (Coulomb Fock term)
+//   G_k    = FFT_{+1}(G_R),  Hee_k = FFT_{+1}(Hee_R)   (Operator::go_to_k)
+// and rho_nn(R=0) of diagonal planes is written to diag0 for the Hartree term.
+// Reference: Functional_SourceTerm.hpp:15-50, kGradient_definitions.hpp:35-40,
+// Coulomb.cpp:150-171, fftPair.cpp:89-107.
+template <bool COUL>
+__global__ void __launch_bounds__(512) plane_rhs_kernel(
+    const double2* __restrict__ rho, long long batch_stride_in, double2* __restrict__ G_out,
+    double2* __restrict__ Hee_out, long long batch_stride_out, const double2* __restrict__ rho0p,
+    const double* __restrict__ Wp, double2* __restrict__ diag0, const StageField* __restrict__ field,
+    const double2* __restrict__ roots, const double* __restrict__ rpos, PlanePlan pl, int nb, double inv_nk) {
+    extern __shared__ double2 smem[];
+    const int Nk = pl.Nk;
+    double2* X = smem;
+    double2* Y = smem + Nk;
+    const int p = blockIdx.x;
+    const int b = blockIdx.y;
+    const double2* src = rho + (long long)b * batch_stride_in + (long long)p * Nk;
+    for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
+    __syncthreads();
+    plane_forward<1>(X, 0, pl, roots);
+
+    const StageField F = field[b];
+    const int n = p / nb, m = p - (p / nb) * nb;
+    if (COUL && n == m && threadIdx.x == 0) diag0[b * nb + n] = cscale(X[0], inv_nk);
+    __syncthreads();  // X[0] is read above before being overwritten below
+    const int n1 = pl.ax[1].n, n2 = pl.ax[2].n;
+    const double* rp0 = rpos + pl.ax[0].rposoff;
+    const double* rp1 = rpos + pl.ax[1].rposoff;
+    const double* rp2 = rpos + pl.ax[2].rposoff;
+    const double2* r0p = rho0p + (long long)p * Nk;
+    const double* wp = Wp + (long long)p * Nk;
+    for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
+        const int q2 = j % n2;
+        const int t = j / n2;
+        const int q1 = t % n1;
+        const int q0 = t / n1;
+        const double dot = F.g[0] * __ldg(&rp0[q0]) + F.g[1] * __ldg(&rp1[q1]) + F.g[2] * __ldg(&rp2[q2]);
+        const double2 r = cscale(X[j], inv_nk);
+        X[j] = make_double2(-dot * r.y, dot * r.x);
+        if (COUL) {
+            const double2 r0 = __ldg(&r0p[j]);
+            const double w = __ldg(&wp[j]);
+            Y[j] = make_double2(-w * (r.x - r0.x), -w * (r.y - r0.y));
+        }
+    }
+    __syncthreads();
+    if (COUL) plane_inverse<2>(X, Nk, pl, roots);
+    else plane_inverse<1>(X, 0, pl, roots);
+
+    double2* gdst = G_out + (long long)b * batch_stride_out + (long long)p * Nk;
+    for (int i = threadIdx.x; i < Nk; i += blockDim.x) gdst[i] = X[i];
+    if (COUL) {
+        double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
+        for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = Y[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Commutator kernel: one CTA per (tile of TK consecutive k, solve b).
+//   H_k  = H0_k + sum_d E_d xi_d,k [+ Hee_k + diag(h)],
+//          h_n = sum_m Hartree_nm (rho_mm(R=0) - rho0_mm(R=0))
+//   f_k  = G_k - i (H_k rho_k - rho_k H_k)
+// then the stage epilogue (mode):
+//   MODE_RHS : out = f
+//   MODE_RK1 : aux = y + h/2 f ; acc = y + h/6 f
+//   MODE_RK2 : aux = y + h/2 f ; acc = acc + h/3 f
+//   MODE_RK3 : aux = y + h f   ; acc = acc + h/3 f
+//   MODE_RK4 : y   = acc + h/6 f
+//   MODE_AB  : hist0 = f ; y = y + c0 f + c1 hist1 + ... (order terms, in sequence)
+// Reference: BlockMatrix_definitions.hpp:203-226 (commutator), Simulation.cpp:335-347
+// (H assembly), Coulomb.cpp:151-159 (Hartree), DESolver.hpp:154-220 (stages).
+enum StageMode { MODE_RHS = 0, MODE_RK1 = 1, MODE_RK2 = 2, MODE_RK3 = 3, MODE_RK4 = 4, MODE_AB = 5 };
+
+struct StageArgs {
+    const double2* rho;   // stage input, [B][P][Nk]
+    const double2* G;     // gradient term in k
+    const double2* Hee;   // HSEX self-energy in k (COUL)
+    const double2* H0;    // [P][Nk]
+    const double2* xi[3]; // [P][Nk]
+    const double2* hartree;    // [P]
+    const double2* rho0diag;   // [nb]  rho0_nn(R=0)
+    const double2* diag0;      // [B][nb] rho_nn(R=0) of the stage input
+    const StageField* field;   // [B]
+    double2* out;   // MODE_RHS
+    double2* y;
+    double2* aux;
+    double2* acc;
+    double2* hist[5];  // AB: hist[0] receives f, hist[i] holds f_{n-i}
+    double c[5];       // AB: h*beta_i; RK: c[0] = stage coefficient for aux, c[1] for acc
+    int order;
+    long long bstride;  // P*Nk
+    int Nk, nb, TK;
+};
+
+template <int MODE, bool COUL>
+__global__ void __launch_bounds__(256) commutator_kernel(StageArgs a) {
+    extern __shared__ double2 sm[];
+    const int nb = a.nb, P = nb * nb, TK = a.TK, Nk = a.Nk;
+    double2* Hs = sm;            // [P][TK]
+    double2* Rs = sm + P * TK;   // [P][TK]
+    double2* hh = Rs + P * TK;   // [nb] Hartree shift
+    const int b = blockIdx.y;
+    const int k0 = blockIdx.x * TK;
+    const long long boff = (long long)b * a.bstride;
+    const StageField F = a.field[b];
+    if (COUL) {
+        for (int n = threadIdx.x; n < nb; n += blockDim.x) {
+            double2 s = make_double2(0.0, 0.0);
+            for (int m = 0; m < nb; ++m) {
+                const double2 d0 = a.diag0[b * nb + m];
+                const double2 r0 = a.rho0diag[m];
+                s = cadd(s, cmul(a.hartree[n * nb + m], csub(d0, r0)));
+            }
+            hh[n] = s;
+        }
+        __syncthreads();
+    }
+    const bool e0 = F.E[0] != 0.0, e1 = F.E[1] != 0.0, e2 = F.E[2] != 0.0;
+    for (int idx = threadIdx.x; idx < P * TK; idx += blockDim.x) {
+        const int p = idx / TK, kk = idx - (idx / TK) * TK;
+        const int k = k0 + kk;
+        double2 h = make_double2(0.0, 0.0), r = make_double2(0.0, 0.0);
+        if (k < Nk) {
+            const long long e = (long long)p * Nk + k;
+            r = __ldg(&a.rho[boff + e]);
+            h = __ldg(&a.H0[e]);
+            if (e0) { double2 x = __ldg(&a.xi[0][e]); h.x += F.E[0] * x.x; h.y += F.E[0] * x.y; }
+            if (e1) { double2 x = __ldg(&a.xi[1][e]); h.x += F.E[1] * x.x; h.y += F.E[1] * x.y; }
+            if (e2) { double2 x = __ldg(&a.xi[2][e]); h.x += F.E[2] * x.x; h.y += F.E[2] * x.y; }
+            if (COUL) {
+                h = cadd(h, __ldg(&a.Hee[boff + e]));
+                const int n = p / nb;
+                if (p == n * nb + n) h = cadd(h, hh[n]);
+            }
+        }
+        Hs[idx] = h;
+        Rs[idx] = r;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < P * TK; idx += blockDim.x) {
+        const int p = idx / TK, kk = idx - (idx / TK) * TK;
+        const int k = k0 + kk;
+        if (k >= Nk) continue;
+        const int i = p / nb, j = p - (p / nb) * nb;
+        double cr = 0.0, ci = 0.0;  // C = H rho - rho H
+        for (int l = 0; l < nb; ++l) {
+            const double2 hil = Hs[(i * nb + l) * TK + kk];
+            const double2 rlj = Rs[(l * nb + j) * TK + kk];
+            const double2 ril = Rs[(i * nb + l) * TK + kk];
+            const double2 hlj = Hs[(l * nb + j) * TK + kk];
+            cr = fma(hil.x, rlj.x, cr);
+            cr = fma(-hil.y, rlj.y, cr);
+            ci = fma(hil.x, rlj.y, ci);
+            ci = fma(hil.y, rlj.x, ci);
+            cr = fma(-ril.x, hlj.x, cr);
+            cr = fma(ril.y, hlj.y, cr);
+            ci = fma(-ril.x, hlj.y, ci);
+            ci = fma(-ril.y, hlj.x, ci);
+        }
+        const long long e = boff + (long long)p * Nk + k;
+        const double2 g = __ldg(&a.G[e]);
+        // f = G - i C
+        const double2 f = make_double2(g.x + ci, g.y - cr);
+        if (MODE == MODE_RHS) {
+            a.out[e] = f;
+        } else if (MODE == MODE_RK1) {
+            const double2 y = a.y[e];
+            a.aux[e] = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
+            a.acc[e] = make_double2(y.x + a.c[1] * f.x, y.y + a.c[1] * f.y);
+        } else if (MODE == MODE_RK2 || MODE == MODE_RK3) {
+            const double2 y = a.y[e];
+            const double2 ac = a.acc[e];
+            a.aux[e] = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
+            a.acc[e] = make_double2(ac.x + a.c[1] * f.x, ac.y + a.c[1] * f.y);
+        } else if (MODE == MODE_RK4) {
+            const double2 ac = a.acc[e];
+            a.y[e] = make_double2(ac.x + a.c[0] * f.x, ac.y + a.c[0] * f.y);
+        } else if (MODE == MODE_AB) {
+            a.hist[0][e] = f;
+            double2 y = a.y[e];
+            y = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
+            for (int q = 1; q < a.order; ++q) {
+                const double2 fq = a.hist[q][e];
+                y = make_double2(y.x + a.c[q] * fq.x, y.y + a.c[q] * fq.y);
+            }
+            a.y[e] = y;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Layout transposes between the reference's [k][p] and the plane-major [p][k].
+__global__ void transpose_kp_to_pk(const double2* __restrict__ src, double2* __restrict__ dst, int Nk, int P) {
+    __shared__ double2 tile[32][33];
+    const int k0 = blockIdx.x * 32, p0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int k = k0 + r, p = p0 + threadIdx.x;
+        if (k < Nk && p < P) tile[r][threadIdx.x] = src[(long long)k * P + p];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int p = p0 + r, k = k0 + threadIdx.x;
+        if (k < Nk && p < P) dst[(long long)p * Nk + k] = tile[threadIdx.x][r];
+    }
+}
+
+__global__ void transpose_pk_to_kp(const double2* __restrict__ src, double2* __restrict__ dst, int Nk, int P) {
+    __shared__ double2 tile[32][33];
+    const int p0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int p = p0 + r, k = k0 + threadIdx.x;
+        if (k < Nk && p < P) tile[r][threadIdx.x] = src[(long long)p * Nk + k];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int k = k0 + r, p = p0 + threadIdx.x;
+        if (k < Nk && p < P) dst[(long long)k * P + p] = tile[threadIdx.x][r];
+    }
+}
+
+// Wannier-gauge population: out[n] = (1/Nk) sum_k Re rho_nn(k), one CTA per n,
+// fixed-order tree reduction (deterministic).
+__global__ void population_kernel(const double2* __restrict__ rho, int Nk, int nb, double* __restrict__ out) {
+    __shared__ double red[256];
+    const int n = blockIdx.x;
+    const double2* plane = rho + (long long)(n * nb + n) * Nk;
+    double s = 0.0;
+    for (int k = threadIdx.x; k < Nk; k += blockDim.x) s += plane[k].x;
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[n] = red[0] / (double)Nk;
+}
+
+// Non-finite detector over a state array: sets *flag to 1 if any component is
+// NaN or Inf.
+__global__ void finite_check_kernel(const double2* __restrict__ x, long long n, int* __restrict__ flag) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double2 v = x[i];
+        if (!isfinite(v.x) || !isfinite(v.y)) {
+            *flag = 1;
+            return;
+        }
+    }
+}
+
+}  // namespace edus

@@ -1,0 +1,285 @@
+"""ctypes host layer over the C ABI of include/edus_gpu.h.
+
+``Solver`` mirrors the reference's ``DESolver<Operator<complex<double>>>``
+call surface (src/DESolver/DESolver.hpp:26-82): ``Propagate``,
+``get_CurrentTime``, ``get_ResolutionTime``, ``get_Function``, plus
+``rhs`` = one ``SourceTerm`` evaluation (Functional_SourceTerm.hpp:10-56).
+Arrays are numpy complex128 in the reference layout [k][n][m].
+
+There is no CPU path: if the CUDA library is missing or fails to load, every
+entry raises ``EdusError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libedus_gpu.so")
+
+EDUS_OK = 0
+ERRORS = {1: "EDUS_ERR_ARG", 2: "EDUS_ERR_CUDA", 3: "EDUS_ERR_TIMEOUT", 4: "EDUS_ERR_DIVERGED",
+          5: "EDUS_ERR_UNSUPPORTED", 6: "EDUS_ERR_NOMEM"}
+SOLVER_AB, SOLVER_RK = 0, 1
+PREC_FP64 = 0
+ENVELOPE_SIN2, ENVELOPE_GAUSS = 0, 1
+
+# every entry point of include/edus_gpu.h
+EXPORTS = [
+    "edus_create", "edus_destroy", "edus_last_error", "edus_upload_model", "edus_set_lasers",
+    "edus_set_state", "edus_get_state", "edus_set_time", "edus_get_time", "edus_rhs", "edus_step",
+    "edus_synchronize", "edus_population_wannier", "edus_device_bytes", "edus_kernel_launches",
+    "edus_get_stream", "edus_set_profiling", "edus_get_profile",
+]
+
+
+class EdusError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _Desc(ctypes.Structure):
+    _fields_ = [("grid", ctypes.c_int * 3), ("nbands", ctypes.c_int), ("solver", ctypes.c_int),
+                ("order", ctypes.c_int), ("dt", ctypes.c_double), ("coulomb", ctypes.c_int),
+                ("precision", ctypes.c_int), ("batch", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+class _Laser(ctypes.Structure):
+    _fields_ = [("intensity", ctypes.c_double), ("omega", ctypes.c_double), ("pol", ctypes.c_double * 3),
+                ("cycles", ctypes.c_double), ("t0", ctypes.c_double), ("phase", ctypes.c_double),
+                ("fwhm", ctypes.c_double), ("envelope", ctypes.c_int)]
+
+
+@dataclass
+class Laser:
+    """One pulse in atomic units (see edus_laser in include/edus_gpu.h)."""
+    intensity: float
+    omega: float
+    pol: tuple
+    cycles: float = 0.0
+    t0: float = 0.0
+    phase: float = 0.0
+    fwhm: float = 0.0
+    envelope: int = ENVELOPE_SIN2
+
+
+_lib = None
+
+
+def load_library(path: str | None = None):
+    """Load libedus_gpu.so (raises EdusError when absent: no fallback)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise EdusError(2, f"CUDA library not built: {p} (run edus_2.0_b200/build.py)")
+    try:
+        L = ctypes.CDLL(p)
+    except OSError as e:  # pragma: no cover - depends on the box
+        raise EdusError(2, f"cannot load {p}: {e}") from e
+    P = ctypes.POINTER
+    dp = P(ctypes.c_double)
+    h = ctypes.c_void_p
+    L.edus_create.argtypes = [P(_Desc), P(h)]
+    L.edus_destroy.argtypes = [h]
+    L.edus_last_error.argtypes = [h]
+    L.edus_last_error.restype = ctypes.c_char_p
+    L.edus_upload_model.argtypes = [h, dp, dp, dp, dp, dp, dp]
+    L.edus_set_lasers.argtypes = [h, ctypes.c_int, ctypes.c_int, P(_Laser)]
+    L.edus_set_state.argtypes = [h, ctypes.c_int, dp]
+    L.edus_get_state.argtypes = [h, ctypes.c_int, dp]
+    L.edus_set_time.argtypes = [h, ctypes.c_double]
+    L.edus_get_time.argtypes = [h, dp]
+    L.edus_rhs.argtypes = [h, ctypes.c_double, dp, dp]
+    L.edus_step.argtypes = [h, ctypes.c_int]
+    L.edus_synchronize.argtypes = [h]
+    L.edus_population_wannier.argtypes = [h, ctypes.c_int, dp]
+    L.edus_device_bytes.argtypes = [h, P(ctypes.c_ulonglong)]
+    L.edus_kernel_launches.argtypes = [h, P(ctypes.c_ulonglong)]
+    L.edus_get_stream.argtypes = [h, P(ctypes.c_void_p)]
+    L.edus_set_profiling.argtypes = [h, ctypes.c_int]
+    L.edus_get_profile.argtypes = [h, ctypes.c_int, dp, P(ctypes.c_ulonglong)]
+    for name in EXPORTS:
+        if name != "edus_last_error":
+            getattr(L, name).restype = ctypes.c_int
+    if path is None:
+        _lib = L
+    return L
+
+
+def _dp(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _c128(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    if shape is not None and a.shape != tuple(shape):
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+class Solver:
+    """GPU counterpart of DESolver<Operator<complex<double>>> for one model.
+
+    grid      : (N0, N1, N2) k grid
+    nbands    : nb
+    solver    : SOLVER_RK or SOLVER_AB ; order 4 (RK) or 4/5 (AB)
+    dt        : ResolutionTime in a.u.
+    coulomb   : include the HSEX self-energy
+    batch     : number of independent solves sharing the model
+    """
+
+    def __init__(self, grid, nbands, dt, solver=SOLVER_RK, order=4, coulomb=False, batch=1, device=0,
+                 precision=PREC_FP64):
+        self._L = load_library()
+        d = _Desc()
+        for i in range(3):
+            d.grid[i] = int(grid[i])
+        d.nbands = int(nbands)
+        d.solver = int(solver)
+        d.order = int(order)
+        d.dt = float(dt)
+        d.coulomb = int(bool(coulomb))
+        d.precision = int(precision)
+        d.batch = int(batch)
+        d.device = int(device)
+        self._h = ctypes.c_void_p()
+        rc = self._L.edus_create(ctypes.byref(d), ctypes.byref(self._h))
+        if rc != EDUS_OK:
+            raise EdusError(rc, self._L.edus_last_error(None).decode())
+        self.grid = tuple(int(x) for x in grid)
+        self.nb = int(nbands)
+        self.Nk = self.grid[0] * self.grid[1] * self.grid[2]
+        self.batch = int(batch)
+        self.dt = float(dt)
+        self.coulomb = bool(coulomb)
+
+    # -- plumbing -----------------------------------------------------------
+    def _check(self, rc):
+        if rc != EDUS_OK:
+            raise EdusError(rc, self._L.edus_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.edus_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        return (self.Nk, self.nb, self.nb)
+
+    # -- model / lasers / state ---------------------------------------------
+    def upload_model(self, H0k, xik, lattice, W=None, rho0R=None, hartree=None):
+        H0k = _c128(H0k, self.shape)
+        xik = _c128(xik, (3,) + self.shape)
+        lat = np.ascontiguousarray(lattice, dtype=np.float64).reshape(3, 3)
+        Wc = _c128(W, self.shape) if W is not None else None
+        r0 = _c128(rho0R, self.shape) if rho0R is not None else None
+        hc = _c128(hartree, (self.nb, self.nb)) if hartree is not None else None
+        self._check(self._L.edus_upload_model(self._h, _dp(H0k), _dp(xik), _dp(lat), _dp(Wc), _dp(r0), _dp(hc)))
+
+    def set_lasers(self, lasers, b=0):
+        arr = (_Laser * max(1, len(lasers)))()
+        for i, L in enumerate(lasers):
+            arr[i].intensity = L.intensity
+            arr[i].omega = L.omega
+            for j in range(3):
+                arr[i].pol[j] = L.pol[j]
+            arr[i].cycles = L.cycles
+            arr[i].t0 = L.t0
+            arr[i].phase = L.phase
+            arr[i].fwhm = L.fwhm
+            arr[i].envelope = L.envelope
+        self._check(self._L.edus_set_lasers(self._h, int(b), len(lasers), arr))
+
+    def set_state(self, rho, b=0):
+        a = _c128(rho, self.shape)
+        self._check(self._L.edus_set_state(self._h, int(b), _dp(a)))
+
+    def get_state(self, b=0, out=None):
+        a = out if out is not None else np.empty(self.shape, dtype=np.complex128)
+        self._check(self._L.edus_get_state(self._h, int(b), _dp(a)))
+        return a
+
+    # DESolver names
+    def get_Function(self, b=0):
+        return self.get_state(b)
+
+    @property
+    def time(self) -> float:
+        t = ctypes.c_double()
+        self._check(self._L.edus_get_time(self._h, ctypes.byref(t)))
+        return t.value
+
+    @time.setter
+    def time(self, t):
+        self._check(self._L.edus_set_time(self._h, float(t)))
+
+    def get_CurrentTime(self):
+        return self.time
+
+    def get_ResolutionTime(self):
+        return self.dt
+
+    # -- compute ------------------------------------------------------------
+    def rhs(self, t, rho):
+        a = _c128(rho, self.shape)
+        out = np.empty(self.shape, dtype=np.complex128)
+        self._check(self._L.edus_rhs(self._h, float(t), _dp(a), _dp(out)))
+        return out
+
+    def step(self, n=1):
+        self._check(self._L.edus_step(self._h, int(n)))
+
+    def Propagate(self, n=1):
+        self.step(n)
+
+    def synchronize(self):
+        self._check(self._L.edus_synchronize(self._h))
+
+    def population_wannier(self, b=0):
+        out = np.empty(self.nb)
+        self._check(self._L.edus_population_wannier(self._h, int(b), _dp(out)))
+        return out
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the handle, as an integer."""
+        v = ctypes.c_void_p()
+        self._check(self._L.edus_get_stream(self._h, ctypes.byref(v)))
+        return v.value or 0
+
+    def set_profiling(self, on: bool):
+        self._check(self._L.edus_set_profiling(self._h, int(bool(on))))
+
+    def profile(self, kind: int):
+        """(total ms, launches) of kernel kind 0 (plane) or 1 (commutator)."""
+        ms = ctypes.c_double()
+        n = ctypes.c_ulonglong()
+        self._check(self._L.edus_get_profile(self._h, int(kind), ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    @property
+    def device_bytes(self) -> int:
+        v = ctypes.c_ulonglong()
+        self._check(self._L.edus_device_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def kernel_launches(self) -> int:
+        v = ctypes.c_ulonglong()
+        self._check(self._L.edus_kernel_launches(self._h, ctypes.byref(v)))
+        return v.value

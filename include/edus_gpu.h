@@ -1,0 +1,166 @@
+/*
+ * edus_gpu.h -- C ABI of the B200 density-matrix propagator.
+ *
+ * The library evaluates the right-hand side
+ *     d rho_k / dt = E(t).grad_k rho_k - i [H0(k) + E(t).xi(k) + H_ee(k), rho_k]
+ * and advances it with RK4 or Adams-Bashforth 4/5 on one GPU.  It replaces
+ * the reference's DESolver<Operator<complex<double>>> + SourceTerm pair
+ * (gcistaro/EDUS_2.0):
+ *     src/DESolver/DESolver.hpp:26-82      DESolver call surface
+ *     src/DESolver/DESolver.hpp:154-220    Propagate_RK / Propagate_AB
+ *     src/Simulation/Functional_SourceTerm.hpp:10-56   SourceTerm
+ *     src/Simulation/Simulation.cpp:163-174            how Simulation wires them
+ *
+ * Conventions shared with the reference:
+ *   - complex numbers are interleaved (re, im) doubles;
+ *   - a k-space operator is row-major [k][n][m], k = i2 + N2*(i1 + N1*i0)
+ *     (src/MeshGrid/MeshGrid.cpp:117-139, BlockMatrix.hpp:48), exactly the
+ *     memory of BlockMatrix<complex<double>>::Values;
+ *   - an R-space operator uses the same index with the FFT output index of the
+ *     k->R transform; R is Gamma-centred ([-N/2, N/2) per axis,
+ *     MeshGrid.cpp:458-486);
+ *   - all quantities are in Hartree atomic units.
+ *
+ * Errors: every entry point returns an int status (EDUS_OK = 0).  No C++
+ * exception crosses this boundary.  edus_last_error() gives a message.
+ * A handle is not thread-safe; distinct handles may be used from distinct
+ * threads.  Work is queued on the handle's own CUDA stream and is complete
+ * when a call that returns host data (edus_get_state, edus_rhs,
+ * edus_observables) or edus_synchronize returns.
+ */
+#ifndef EDUS_GPU_H
+#define EDUS_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EDUS_OK 0
+#define EDUS_ERR_ARG 1         /* invalid argument or call order */
+#define EDUS_ERR_CUDA 2        /* CUDA runtime error (message has details) */
+#define EDUS_ERR_TIMEOUT 3     /* a bounded device wait ran out */
+#define EDUS_ERR_DIVERGED 4    /* non-finite density matrix detected */
+#define EDUS_ERR_UNSUPPORTED 5 /* size or option this build does not handle */
+#define EDUS_ERR_NOMEM 6       /* device allocation failed */
+
+/* SolverType, src/Constants.hpp:27 (AB = 0, RK = 1) */
+#define EDUS_SOLVER_AB 0
+#define EDUS_SOLVER_RK 1
+
+/* Arithmetic of the right-hand side.  FP64 is the drop-in form. */
+#define EDUS_PREC_FP64 0
+
+/* Laser envelopes.  SIN2 is the reference's pulse (src/Laser/Laser.cpp:96-134):
+ *   E(t) = sqrt(I) sin^2(pi (t-t0)/(cycles*T)) sin(w (t-t0) + phase) pol,
+ *   zero for t-t0 <= 1e-7 or t-t0 > cycles*T.
+ * GAUSS is an extension (no reference counterpart):
+ *   E(t) = sqrt(I) exp(-2 ln2 (t-t0)^2 / fwhm^2) cos(w (t-t0) + phase) pol,
+ *   fwhm being the full width at half maximum of the intensity. */
+#define EDUS_ENVELOPE_SIN2 0
+#define EDUS_ENVELOPE_GAUSS 1
+
+typedef struct edus_handle edus_handle;
+
+typedef struct {
+    int grid[3];     /* N0, N1, N2 of the k grid (= the R grid) */
+    int nbands;      /* nb: rows/cols of each block */
+    int solver;      /* EDUS_SOLVER_RK or EDUS_SOLVER_AB */
+    int order;       /* 4 for RK; 4 or 5 for AB */
+    double dt;       /* DESolver::ResolutionTime, a.u. */
+    int coulomb;     /* 1: add the HSEX self-energy (Coulomb::EffectiveHamiltonian) */
+    int precision;   /* EDUS_PREC_FP64 */
+    int batch;       /* independent solves sharing one model (>= 1) */
+    int device;      /* CUDA device ordinal */
+} edus_desc;
+
+typedef struct {
+    double intensity;  /* a.u. (amplitude = sqrt(intensity)) */
+    double omega;      /* a.u. */
+    double pol[3];     /* Cartesian; normalised by the library */
+    double cycles;     /* SIN2: duration in optical periods */
+    double t0;         /* SIN2: start time; GAUSS: centre, a.u. */
+    double phase;      /* carrier phase, rad */
+    double fwhm;       /* GAUSS: intensity FWHM, a.u. */
+    int envelope;      /* EDUS_ENVELOPE_* */
+} edus_laser;
+
+/* Create a handle and allocate every device buffer it will use.
+ * Replaces DESolver::initialize + Operator::initialize_fft
+ * (src/DESolver/DESolver.cpp:11-33, src/Operator/Operator.hpp:192-252). */
+int edus_create(const edus_desc* desc, edus_handle** out);
+
+/* Release the handle and its device memory. */
+int edus_destroy(edus_handle* h);
+
+/* Message of the last failure on this handle (or of the last failed
+ * edus_create when h is NULL).  Never NULL. */
+const char* edus_last_error(const edus_handle* h);
+
+/* Upload the model (host buffers, caller-owned, copied during the call).
+ *   H0_k   [Nk][nb][nb]    H0(k), Simulation::H0_ (Simulation.cpp:99-118)
+ *   xi_k   [3][Nk][nb][nb] r_d(k), the Wannier position operator made
+ *                          Hermitian (Simulation.cpp:93-97)
+ *   lattice[9]             A, row-major, lattice vectors in the COLUMNS,
+ *                          bohr (src/Model/Model.hpp:41-44)
+ *   W_R    [Nk][nb][nb]    screened potential on the R grid
+ *                          (ModelCoulomb::ScreenedPotential_); NULL if coulomb=0
+ *   rho0_R [Nk][nb][nb]    ground-state density in R (Coulomb::DM0_); NULL if coulomb=0
+ *   hartree[nb][nb]        Coulomb::Hartree (Coulomb.cpp:41-58); NULL if coulomb=0
+ * The gradient term uses R.E with R = A R_crys, R_crys Gamma-centred
+ * (kGradient_definitions.hpp:35-40). */
+int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k,
+                      const double* lattice, const double* W_R, const double* rho0_R,
+                      const double* hartree);
+
+/* Lasers of solve `b` (0 <= b < batch).  Replaces SetOfLaser
+ * (src/Laser/Laser.hpp:128-170).  n may be 0 (no field). */
+int edus_set_lasers(edus_handle* h, int b, int n, const edus_laser* lasers);
+
+/* Density matrix of solve b in k, [Nk][nb][nb] (DESolver::get_Function). */
+int edus_set_state(edus_handle* h, int b, const double* rho_k);
+int edus_get_state(edus_handle* h, int b, double* rho_k);
+
+/* DESolver::CurrentTime.  Like the reference, it starts at 0 whatever the
+ * initial time (DESolver.hpp:36, set_InitialTime does not move it). */
+int edus_set_time(edus_handle* h, double t);
+int edus_get_time(const edus_handle* h, double* t);
+
+/* One SourceTerm evaluation of solve 0 at time t (the field is taken from the
+ * lasers of solve 0): out_k = f(t, in_k).  Host buffers [Nk][nb][nb].
+ * Replaces Functional_SourceTerm.hpp:10-56. */
+int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k);
+
+/* Advance every solve by n steps (DESolver::Propagate(n), DESolver.hpp:238-242).
+ * Asynchronous: returns once the work is queued. */
+int edus_step(edus_handle* h, int n);
+
+/* Wait for queued work; reports device-side errors. */
+int edus_synchronize(edus_handle* h);
+
+/* Observables of solve b for the current state, as Simulation::do_onestep
+ * prints them (Simulation.cpp:439-470, 583-622):
+ *   pop_wannier[nb] = (1/Nk) sum_k Re rho_nn(k).
+ * Requires no extra model data. */
+int edus_population_wannier(edus_handle* h, int b, double* pop_wannier);
+
+/* The CUDA stream (cudaStream_t) every kernel of this handle runs on. */
+int edus_get_stream(const edus_handle* h, void** stream);
+
+/* Per-kernel timing with CUDA events on the handle's stream (off by default).
+ * kind 0 = plane kernel (k<->R transforms + gradient + HSEX), 1 = commutator
+ * + stage kernel.  Totals accumulate from the call that enabled profiling;
+ * edus_get_profile synchronises the stream. */
+int edus_set_profiling(edus_handle* h, int on);
+int edus_get_profile(edus_handle* h, int kind, double* total_ms, unsigned long long* launches);
+
+/* Size in bytes of the device memory the handle holds. */
+int edus_device_bytes(const edus_handle* h, unsigned long long* bytes);
+
+/* Number of kernel launches this handle has queued since creation. */
+int edus_kernel_launches(const edus_handle* h, unsigned long long* n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EDUS_GPU_H */

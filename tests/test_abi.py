@@ -1,0 +1,61 @@
+"""The C-ABI library: builds for sm_100a, loads, and exports every entry point
+that include/edus_gpu.h declares.  No compute call is made here (CPU only)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def declared_entry_points():
+    src = open(os.path.join(ROOT, "include", "edus_gpu.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(edus_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_header_lists_entry_points():
+    names = declared_entry_points()
+    assert "edus_create" in names and "edus_step" in names and "edus_rhs" in names
+    assert len(names) >= 10
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    lib = pkg.edus.load_library()
+    missing = [n for n in declared_entry_points() if not hasattr(lib, n)]
+    assert not missing, missing
+    # the binding's own list covers the header exactly
+    assert sorted(pkg.edus.EXPORTS) == declared_entry_points()
+
+
+def test_library_is_sm100a_build(pkg):
+    # the build step always targets sm_100a only
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("edus_build", os.path.join(ROOT, "edus_2.0_b200", "build.py"))
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    assert b.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert os.path.exists(b.LIB)
+
+
+def test_create_rejects_bad_arguments_without_gpu(pkg):
+    # argument checks run before any CUDA call, so they work on a CPU-only box
+    E = pkg.edus
+    with pytest.raises(E.EdusError) as ei:
+        E.Solver((4, 4, 1), 2, dt=-1.0)
+    assert ei.value.code == 1
+    with pytest.raises(E.EdusError) as ei:
+        E.Solver((4, 4, 1), 2, dt=0.1, solver=E.SOLVER_RK, order=5)
+    assert ei.value.code == 5
+    with pytest.raises(E.EdusError) as ei:
+        E.Solver((0, 4, 1), 2, dt=0.1)
+    assert ei.value.code == 1
+
+
+def test_no_cpu_fallback(pkg, tmp_path):
+    # a missing library raises instead of falling back to any CPU path
+    E = pkg.edus
+    with pytest.raises(E.EdusError):
+        E.load_library(str(tmp_path / "missing.so"))
