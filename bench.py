@@ -59,12 +59,21 @@ class ClockSampler:
         self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
 
     def __enter__(self):
+        self.err = tempfile.NamedTemporaryFile("w+", suffix=".err", delete=False)
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.out, stderr=self.err)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return self
+        # start timing only once the sampler produces rows
+        t0 = time.time()
+        while time.time() - t0 < 5.0:
+            self.out.flush()
+            if os.path.getsize(self.out.name) > 0:
+                break
+            time.sleep(0.05)
         return self
 
     def __exit__(self, *a):
@@ -85,7 +94,13 @@ class ClockSampler:
                     rows.append(parts)
         os.unlink(self.out.name)
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+            err = ""
+            try:
+                with open(self.err.name) as f:
+                    err = f.read().strip()[:200]
+            except OSError:
+                pass
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0, "error": err}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -104,19 +119,19 @@ def measured_peaks():
 
 
 def algorithmic_bytes(P, Nk, B, d_E, coulomb=True):
-    """Algorithmic HBM bytes of one RK4 step's launches (FP64, 16 B complex).
+    """Algorithmic HBM bytes (FP64, 16 B per complex number).
 
-    plane kernel, per plane: read rho_s, write G; HSEX adds read rho0, read W
-    (real, 8 B), write Hee.
-    commutator kernel, per element: read rho_s, G, H0, d_E*xi [, Hee] and the
-    stage bookkeeping: RK1 writes aux, acc; RK2/3 read y, acc and write aux,
-    acc; RK4 reads acc and writes y."""
+    plane kernel, per launch (one right-hand side, every plane of every solve):
+      read rho_s, write G; HSEX adds read rho0, read W (real, 8 B), write Hee.
+    commutator kernel, per launch, stage s of RK4: read rho_s, G, H0, d_E*xi
+      [, Hee]; RK1 writes aux, acc; RK2/3 also read y, acc; RK4 reads acc and
+      writes y.
+    Returns (plane bytes per launch, [commutator bytes of RK stage 1..4])."""
     c = 16.0
-    plane = P * Nk * ((2 * c) + ((c + 8 + c) if coulomb else 0)) * B
+    plane = P * Nk * (2 * c + ((c + 8 + c) if coulomb else 0)) * B
     common = c * (3 + d_E + (1 if coulomb else 0))
-    comm = [common + 2 * c, common + 4 * c, common + 4 * c, common + 2 * c]
-    comm_total = sum(P * Nk * x for x in comm) * B
-    return plane, comm_total
+    comm = [P * Nk * B * x for x in (common + 2 * c, common + 4 * c, common + 4 * c, common + 2 * c)]
+    return plane, comm
 
 
 def run_ours(args, rank, world, local_rank):
@@ -186,15 +201,17 @@ def run_ours(args, rank, world, local_rank):
     P, Nk = model.nb ** 2, model.Nk
     pol = np.asarray(cfg.lasers[0].pol, dtype=float)
     d_E = int(np.count_nonzero(pol))
-    plane_B, comm_B = algorithmic_bytes(P, Nk, B, d_E, cfg.coulomb)
+    plane_launch_B, comm_stage_B = algorithmic_bytes(P, Nk, B, d_E, cfg.coulomb)
+    comm_launch_B = sum(comm_stage_B) / 4.0
+    step_B = 4 * plane_launch_B + sum(comm_stage_B)
     plane_avg = plane_ms / max(plane_n, 1)
     comm_avg = comm_ms / max(comm_n, 1)
     peak, peak_kind = measured_peaks()
     dominant = "plane_rhs_kernel" if plane_ms >= comm_ms else "commutator_kernel"
     if dominant == "plane_rhs_kernel":
-        ach = plane_B / 4 / (plane_avg / 1e3) / 1e9
+        ach = plane_launch_B / (plane_avg / 1e3) / 1e9
     else:
-        ach = comm_B / 4 / (comm_avg / 1e3) / 1e9
+        ach = comm_launch_B / (comm_avg / 1e3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
@@ -241,7 +258,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": f"{WORKLOAD}: 22-orbital TMD-like, 72x72x1 k grid, HSEX (RK r0=40 A, eps=1), "
                                f"RK4 dt=0.005 fs, batch={B} solve(s) per GPU",
                    "batch": B, "l2": f"inputs larger than L2 (state {S_bytes / 1e6:.1f} MB x {B}; "
-                                     f"per-step working set {(plane_B + comm_B) / 1e9:.2f} GB)",
+                                     f"per-step traffic {step_B / 1e9:.2f} GB)",
                    "parallelism": f"replicas x{world}"},
         "gpu_launches": int(launches),
         "clocks": clk,
@@ -249,9 +266,11 @@ def run_ours(args, rank, world, local_rank):
                      "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": traffic,
                      "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
                      "plane_kernel_ms": round(plane_avg, 5), "commutator_kernel_ms": round(comm_avg, 5),
-                     "plane_bytes_per_launch": plane_B / 4, "commutator_bytes_per_launch": comm_B / 4,
-                     "step_bytes": plane_B + comm_B,
-                     "step_GBps": round((plane_B + comm_B) / (ms_max / K / 1e3) / 1e9, 1)},
+                     "plane_bytes_per_launch": plane_launch_B, "commutator_bytes_per_launch": comm_launch_B,
+                     "plane_GBps": round(plane_launch_B / (plane_avg / 1e3) / 1e9, 1),
+                     "commutator_GBps": round(comm_launch_B / (comm_avg / 1e3) / 1e9, 1),
+                     "step_bytes": step_B,
+                     "step_GBps": round(step_B / (ms_max / K / 1e3) / 1e9, 1)},
         "e2e": {"value": round(e2e_value, 3), "unit": "steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "finite": finite},
     }
@@ -318,7 +337,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=1500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--batch", type=int, default=1)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")

@@ -90,18 +90,22 @@ def test_rhs_parity(pkg, po, tmp_path, name, grid, nb, dims, coulomb):
 @pytest.mark.parametrize("solver,order", [("RK", 4), ("AB", 4), ("AB", 5)])
 @pytest.mark.parametrize("coulomb", [False, True])
 def test_steps_parity(pkg, po, tmp_path, solver, order, coulomb):
+    # dt = 0.01 fs keeps AB5 inside its stability region for this model
     inp = model_input(pkg, tmp_path, f"st_{solver}{order}{int(coulomb)}", (10, 9, 1), nb=4, coulomb=coulomb,
-                      solver=solver, order=order, dt=0.1)
+                      solver=solver, order=order, dt=0.01)
     cfg, o, s = make_pair(pkg, po, inp)
-    for chunk in (1, 3, 8):
+    n0 = np.abs(o.get("rho")).max()
+    for chunk in (1, 3, 8, 20):
         s.step(chunk)
         o.step(chunk)
-        assert rel(s.get_state(), o.get("rho")) < TOL
+        ref = o.get("rho")
+        assert np.abs(ref).max() < 10 * n0  # a bounded (physical) trajectory
+        assert rel(s.get_state(), ref) < TOL
         assert s.time == pytest.approx(o.time, rel=0, abs=1e-12)
 
 
 def test_batch_equals_separate_solves(pkg, po, tmp_path):
-    inp = model_input(pkg, tmp_path, "batch", (8, 8, 1), nb=3, coulomb=True, dt=0.1)
+    inp = model_input(pkg, tmp_path, "batch", (8, 8, 1), nb=3, coulomb=True, dt=0.01)
     cfg, o, s = make_pair(pkg, po, inp, batch=3)
     base = lasers_of(pkg, cfg)[0]
     las = []
