@@ -59,3 +59,32 @@ def test_no_cpu_fallback(pkg, tmp_path):
     E = pkg.edus
     with pytest.raises(E.EdusError):
         E.load_library(str(tmp_path / "missing.so"))
+
+
+def test_cpp_facade_compiles_and_links(tmp_path):
+    """include/edus_gpu.hpp (the DESolver-shaped C++ facade) compiles against the
+    header and links against the built library without a GPU."""
+    import shutil
+    import subprocess
+
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no g++")
+    src = tmp_path / "use.cpp"
+    src.write_text(
+        '#include "edus_gpu.hpp"\n'
+        "int main() {\n"
+        "  edus_gpu::GpuDESolver s;\n"
+        "  (void)s;\n"
+        "  edus_desc d{};\n"
+        "  edus_handle* h = nullptr;\n"
+        "  int rc = edus_create(&d, &h);  // invalid descriptor: rejected before any CUDA call\n"
+        "  return rc == EDUS_ERR_ARG ? 0 : 1;\n"
+        "}\n")
+    libdir = os.path.join(ROOT, "edus_2.0_b200", "lib")
+    exe = tmp_path / "use"
+    env = dict(os.environ)
+    env.pop("CXX", None)
+    subprocess.run([gxx, "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-L", libdir, "-ledus_gpu",
+                    f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True, env=env)
+    assert subprocess.run([str(exe)]).returncode == 0
