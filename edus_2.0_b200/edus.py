@@ -32,7 +32,7 @@ EXPORTS = [
     "edus_create", "edus_destroy", "edus_last_error", "edus_upload_model", "edus_set_lasers",
     "edus_set_state", "edus_get_state", "edus_set_time", "edus_get_time", "edus_rhs", "edus_step",
     "edus_synchronize", "edus_population_wannier", "edus_device_bytes", "edus_kernel_launches",
-    "edus_get_stream", "edus_set_profiling", "edus_get_profile",
+    "edus_get_stream", "edus_set_profiling", "edus_get_profile", "edus_rhs_noalloc",
 ]
 
 
@@ -104,6 +104,9 @@ def load_library(path: str | None = None):
     L.edus_get_stream.argtypes = [h, P(ctypes.c_void_p)]
     L.edus_set_profiling.argtypes = [h, ctypes.c_int]
     L.edus_get_profile.argtypes = [h, ctypes.c_int, dp, P(ctypes.c_ulonglong)]
+    vp = ctypes.c_void_p
+    L.edus_rhs_noalloc.argtypes = [P(ctypes.c_int), ctypes.c_int, ctypes.c_int, dp, dp, vp, vp, vp, vp, vp, vp, vp,
+                                   vp, ctypes.c_char_p, ctypes.c_int]
     for name in EXPORTS:
         if name != "edus_last_error":
             getattr(L, name).restype = ctypes.c_int

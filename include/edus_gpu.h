@@ -153,6 +153,42 @@ int edus_get_stream(const edus_handle* h, void** stream);
 int edus_set_profiling(edus_handle* h, int on);
 int edus_get_profile(edus_handle* h, int kind, double* total_ms, unsigned long long* launches);
 
+/* ------------------------------------------------------------------------
+ * No-allocation variant of edus_rhs.  No counterpart in the reference.
+ *
+ * For callers that cannot let a library allocate device memory: their GPU
+ * memory belongs to another allocator (a framework's caching allocator that
+ * reserves the device up front, a fixed pool sized at start-up), or they run
+ * a time-critical loop where cudaMalloc's implicit device-wide
+ * synchronisation is unacceptable.  The caller passes device buffers for all
+ * inputs and the output; the intermediates live in one array built into the
+ * library's CUDA module, EDUS_NOALLOC_SCRATCH_BYTES long, which every GPU that
+ * loads the library holds until the process exits.  Nothing in this call
+ * allocates (no cudaMalloc / cudaFree, no allocating library routine).
+ *
+ *   grid, nbands, coulomb   as in edus_desc
+ *   lattice[9], efield[3]   HOST arrays: A (columns = lattice vectors, bohr)
+ *                           and the field E(t) of this evaluation (a.u.)
+ *   H0_k, xi_k, W_R, rho0_R, hartree
+ *                           DEVICE arrays, layouts of edus_upload_model
+ *                           (W_R, rho0_R, hartree may be NULL if coulomb = 0)
+ *   in_k, out_k             DEVICE arrays [Nk][nb][nb]: out = f(in)
+ *   stream                  cudaStream_t the work is queued on (NULL = legacy)
+ *   errbuf, errlen          optional buffer for a message on failure
+ * Returns once the work is queued.  The intermediates must fit the array
+ * (about 6.5 * Nk * nb^2 * 16 bytes with coulomb, 4 * ... without); larger
+ * problems get EDUS_ERR_UNSUPPORTED.  The first call on a device looks up the
+ * array's address and raises the kernels' shared-memory limit: make it before
+ * any stream capture on that device.  All calls share the array, and each
+ * call overwrites what the last one left there: calls that overlap on the
+ * GPU (several streams or host threads at once) race and must be serialised
+ * by the caller. */
+#define EDUS_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, const double lattice[9],
+                     const double efield[3], const double* H0_k, const double* xi_k,
+                     const double* W_R, const double* rho0_R, const double* hartree,
+                     const double* in_k, double* out_k, void* stream, char* errbuf, int errlen);
+
 /* Size in bytes of the device memory the handle holds. */
 int edus_device_bytes(const edus_handle* h, unsigned long long* bytes);
 
