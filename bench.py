@@ -213,10 +213,13 @@ def run_ours(args, rank, world, local_rank):
     else:
         ach = comm_launch_B / (comm_avg / 1e3) / 1e9
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    tf = os.path.join(ROOT, "profiles", "traffic.txt")  # DRAM bytes per launch from the committed ncu capture
     if os.path.exists(tf):
         with open(tf) as f:
-            traffic = json.load(f).get(dominant)
+            for line in f:
+                parts = line.split()
+                if len(parts) == 2 and not line.startswith("#") and parts[0] == dominant:
+                    traffic = float(parts[1])
 
     # ---- end to end through the public API with host buffers ----
     host_rho = torch.empty((model.Nk, model.nb, model.nb), dtype=torch.complex128).pin_memory()
