@@ -14,6 +14,7 @@
 #include <stdexcept>
 #include "../../include/edus_gpu.h"
 #include "kernels.cuh"
+#include "plane_plan.hpp"
 
 using namespace edus;
 
@@ -39,7 +40,7 @@ struct edus_handle {
     double t = 0.0;
     double A[9] = {0};  // lattice, row-major, vectors in columns
     PlanePlan plan{};
-    int smem_plane = 0, smem_comm = 0, TK = 4;
+    int smem_plane = 0, smem_comm = 0, TK = 4, comm_threads = 256;
     unsigned long long launches = 0;
     size_t dev_bytes = 0;
     std::vector<std::vector<edus_laser>> lasers;
@@ -106,34 +107,6 @@ int dalloc(edus_handle* h, void** p, size_t bytes) {
         if (rc_ != EDUS_OK) return rc_;                           \
     } while (0)
 
-// Radices of one axis in DIF order: powers of two first (8, then 4/2), odd
-// radices last (they sit at the short strides, where odd spacing avoids
-// shared-memory bank conflicts).
-bool factor_axis(int n, std::vector<int>& r) {
-    r.clear();
-    int m = n;
-    while (m % 8 == 0) { r.push_back(8); m /= 8; }
-    if (m % 4 == 0) { r.push_back(4); m /= 4; }
-    if (m % 2 == 0) { r.push_back(2); m /= 2; }
-    for (int q : {3, 5, 7})
-        while (m % q == 0) { r.push_back(q); m /= q; }
-    return m == 1 && (int)r.size() <= kMaxStages;
-}
-
-// frequency index stored at each position after the DIF pass
-void dif_positions(int n, const std::vector<int>& r, std::vector<int>& freq_at_pos) {
-    freq_at_pos.assign(n, 0);
-    for (int k = 0; k < n; ++k) {
-        int pos = 0, len = n, kk = k;
-        for (int radix : r) {
-            len /= radix;
-            pos += (kk % radix) * len;
-            kk /= radix;
-        }
-        freq_at_pos[pos] = k;
-    }
-}
-
 void field_at(const std::vector<edus_laser>& ls, const double A[9], double t, StageField& f) {
     // SetOfLaser::operator() (Laser.hpp:143-150) with Laser::operator()
     // (Laser.cpp:131-134), envelope (Laser.cpp:96-104), carrier (Laser.cpp:35-38)
@@ -162,15 +135,6 @@ void field_at(const std::vector<edus_laser>& ls, const double A[9], double t, St
     }
     for (int d = 0; d < 3; ++d) f.E[d] = E[d];
     for (int c = 0; c < 3; ++c) f.g[c] = A[0 * 3 + c] * E[0] + A[1 * 3 + c] * E[1] + A[2 * 3 + c] * E[2];
-}
-
-int choose_tk(int P) {
-    int tk = 1;
-    while (tk * P < 1024 && tk < 64) tk *= 2;
-    if (tk < 4) tk = 4;
-    // keep the two smem tiles within 64 KB where possible
-    while (tk > 4 && (size_t)2 * P * tk * 16 > 64 * 1024) tk /= 2;
-    return tk;
 }
 
 cudaEvent_t prof_event(edus_handle* h) {
@@ -236,9 +200,9 @@ int launch_comm_mode(edus_handle* h, const StageArgs& a, int nbatch) {
     cudaEvent_t e0;
     prof_begin(h, &e0);
     if (h->d.coulomb)
-        commutator_kernel<MODE, true><<<grid, 256, h->smem_comm, h->stream>>>(a);
+        commutator_kernel<MODE, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
     else
-        commutator_kernel<MODE, false><<<grid, 256, h->smem_comm, h->stream>>>(a);
+        commutator_kernel<MODE, false><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
     h->launches++;
     CU(h, cudaGetLastError());
     prof_end(h, 1, e0);
@@ -324,40 +288,13 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
         return bail(fail(h, EDUS_ERR_CUDA, "cudaStreamCreate failed"));
 
     // FFT plan per axis
-    std::vector<double2> roots;
-    std::vector<double> rpos;
-    int stride = 1;
-    for (int ax = 2; ax >= 0; --ax) {
-        AxisPlan& A = h->plan.ax[ax];
-        A.n = h->N[ax];
-        A.inner = stride;
-        stride *= A.n;
-        std::vector<int> r;
-        if (!factor_axis(A.n, r))
-            return bail(fail(h, EDUS_ERR_UNSUPPORTED, "grid size " + std::to_string(A.n) +
-                                                          " has a prime factor other than 2, 3, 5, 7"));
-        A.nst = (int)r.size();
-        int L = A.n;
-        for (int s = 0; s < A.nst; ++s) {
-            A.r[s] = r[s];
-            L /= r[s];
-            A.L[s] = L;
-        }
-        A.rootoff = (int)roots.size();
-        for (int j = 0; j < A.n; ++j) {
-            long double a = -2.0L * 3.14159265358979323846264338327950288L * j / A.n;
-            roots.push_back(make_double2((double)cosl(a), (double)sinl(a)));
-        }
-        A.rposoff = (int)rpos.size();
-        std::vector<int> fp;
-        dif_positions(A.n, r, fp);
-        for (int q = 0; q < A.n; ++q) {
-            int j = fp[q];
-            // Gamma-centred coordinate, MeshGrid.cpp:352-375 with [-N/2, N/2)
-            rpos.push_back(2 * j >= A.n ? double(j - A.n) : double(j));
-        }
+    PlaneTables tabs;
+    {
+        std::string perr;
+        if (!build_plane_plan(h->N, h->plan, tabs, perr)) return bail(fail(h, EDUS_ERR_UNSUPPORTED, perr));
     }
-    h->plan.Nk = h->Nk;
+    const std::vector<double2>& roots = tabs.roots;
+    const std::vector<double>& rpos = tabs.rpos;
 
     int dev_smem = 0;
     cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, d.device);
@@ -367,8 +304,10 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
                          "k grid of " + std::to_string(h->Nk) + " points does not fit one plane" +
                              (d.coulomb ? " pair" : "") + " in shared memory (" + std::to_string(dev_smem) + " B)"));
     h->smem_plane = (int)plane_bytes;
-    h->TK = choose_tk(h->P);
-    h->smem_comm = (int)((2 * (size_t)h->P * h->TK + h->nb) * sizeof(double2));
+    const CommGeom cg = comm_geometry(h->nb);
+    h->TK = cg.TK;
+    h->comm_threads = cg.threads;
+    h->smem_comm = (int)cg.smem;
     if (h->smem_comm > dev_smem) return bail(fail(h, EDUS_ERR_UNSUPPORTED, "too many bands for the commutator tile"));
     int rc;
     if ((rc = set_smem(h, plane_rhs_kernel<true>, h->smem_plane))) return bail(rc);

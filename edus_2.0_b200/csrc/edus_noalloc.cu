@@ -33,6 +33,7 @@
 // this translation unit carries its own copies.
 namespace {
 #include "kernels.cuh"
+#include "plane_plan.hpp"
 }  // namespace
 
 using namespace edus;
@@ -53,31 +54,6 @@ thread_local int g_errlen = 0;
 int nfail(int code, const std::string& msg) {
     if (g_errbuf && g_errlen > 0) std::snprintf(g_errbuf, (size_t)g_errlen, "%s", msg.c_str());
     return code;
-}
-
-// Same axis factorisation and DIF position order as the handle path.
-bool factor_axis_na(int n, std::vector<int>& r) {
-    r.clear();
-    int m = n;
-    while (m % 8 == 0) { r.push_back(8); m /= 8; }
-    if (m % 4 == 0) { r.push_back(4); m /= 4; }
-    if (m % 2 == 0) { r.push_back(2); m /= 2; }
-    for (int q : {3, 5, 7})
-        while (m % q == 0) { r.push_back(q); m /= q; }
-    return m == 1 && (int)r.size() <= kMaxStages;
-}
-
-void dif_positions_na(int n, const std::vector<int>& r, std::vector<int>& fq) {
-    fq.assign(n, 0);
-    for (int k = 0; k < n; ++k) {
-        int pos = 0, len = n, kk = k;
-        for (int radix : r) {
-            len /= radix;
-            pos += (kk % radix) * len;
-            kk /= radix;
-        }
-        fq[pos] = k;
-    }
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -141,42 +117,15 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
 
     // FFT plan and tables (host), as in edus_create
     PlanePlan plan{};
-    std::vector<double2> roots;
-    std::vector<double> rpos;
-    std::vector<int> fqall;
-    int fqoff[3];
-    int stride = 1;
-    for (int ax = 2; ax >= 0; --ax) {
-        AxisPlan& A = plan.ax[ax];
-        A.n = N[ax];
-        A.inner = stride;
-        stride *= A.n;
-        std::vector<int> r;
-        if (!factor_axis_na(A.n, r))
-            return nfail(EDUS_ERR_UNSUPPORTED, "edus_rhs_noalloc: grid size " + std::to_string(A.n) +
-                                                   " has a prime factor other than 2, 3, 5, 7");
-        A.nst = (int)r.size();
-        int L = A.n;
-        for (int s = 0; s < A.nst; ++s) {
-            A.r[s] = r[s];
-            L /= r[s];
-            A.L[s] = L;
-        }
-        A.rootoff = (int)roots.size();
-        for (int j = 0; j < A.n; ++j) {
-            long double a = -2.0L * 3.14159265358979323846264338327950288L * j / A.n;
-            roots.push_back(make_double2((double)cosl(a), (double)sinl(a)));
-        }
-        A.rposoff = (int)rpos.size();
-        std::vector<int> fq;
-        dif_positions_na(A.n, r, fq);
-        fqoff[ax] = (int)fqall.size();
-        for (int q = 0; q < A.n; ++q) {
-            rpos.push_back(2 * fq[q] >= A.n ? double(fq[q] - A.n) : double(fq[q]));
-            fqall.push_back(fq[q]);
-        }
+    PlaneTables tabs;
+    {
+        std::string perr;
+        if (!build_plane_plan(N, plan, tabs, perr)) return nfail(EDUS_ERR_UNSUPPORTED, "edus_rhs_noalloc: " + perr);
     }
-    plan.Nk = Nk;
+    const std::vector<double2>& roots = tabs.roots;
+    const std::vector<double>& rpos = tabs.rpos;
+    const std::vector<int>& fqall = tabs.fq;
+    const int* fqoff = tabs.fqoff;
 
     // carve the scratch array
     size_t off = 0;
@@ -204,11 +153,9 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
                                                std::to_string((size_t)EDUS_NOALLOC_SCRATCH_BYTES) +
                                                " (use edus_create/edus_rhs)");
     const size_t plane_smem = (size_t)Nk * sizeof(double2) * (coulomb ? 2 : 1);
-    int tk = 1;
-    while (tk * P < 1024 && tk < 64) tk *= 2;
-    if (tk < 4) tk = 4;
-    while (tk > 4 && (size_t)2 * P * tk * 16 > 64 * 1024) tk /= 2;
-    const size_t comm_smem = (2 * (size_t)P * tk + nb) * sizeof(double2);
+    const CommGeom cgeo = comm_geometry(nb);
+    const int tk = cgeo.TK;
+    const size_t comm_smem = cgeo.smem;
 
     // per-device set-up: the array's device address and the kernels' limits
     int dev = 0;
@@ -311,9 +258,9 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
     a.TK = tk;
     dim3 cg((Nk + tk - 1) / tk, 1);
     if (coulomb)
-        commutator_kernel<MODE_RHS, true><<<cg, 256, comm_smem, stream>>>(a);
+        commutator_kernel<MODE_RHS, true><<<cg, cgeo.threads, comm_smem, stream>>>(a);
     else
-        commutator_kernel<MODE_RHS, false><<<cg, 256, comm_smem, stream>>>(a);
+        commutator_kernel<MODE_RHS, false><<<cg, cgeo.threads, comm_smem, stream>>>(a);
     NA_CU(cudaGetLastError());
     dim3 tg2((P + 31) / 32, (Nk + 31) / 32);
     transpose_pk_to_kp<<<tg2, tb, 0, stream>>>(out_pk, (double2*)out_k, Nk, P);

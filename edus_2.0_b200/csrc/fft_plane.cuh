@@ -18,7 +18,24 @@
 
 namespace edus {
 
-constexpr int kMaxStages = 12;
+constexpr int kMaxStages = 8;
+
+// Division by a run-time constant d < 2^16 of x < 2^24 without a divide:
+// q = (x * m) >> 40 with m = ceil(2^40 / d).  The error of x*m/2^40 against
+// x/d is below x/2^40 < 2^-16 < 1/d, so the floor is exact.
+struct FastDiv {
+    unsigned long long m;
+    int d;
+};
+inline FastDiv make_fastdiv(int d) {
+    FastDiv f;
+    f.d = d;
+    f.m = ((1ull << 40) + (unsigned long long)d - 1ull) / (unsigned long long)d;
+    return f;
+}
+__device__ __forceinline__ int fdiv(int x, const FastDiv& f) {
+    return (int)(((unsigned long long)(unsigned)x * f.m) >> 40);
+}
 
 struct AxisPlan {
     int n;        // length along the axis (1 = axis absent)
@@ -28,11 +45,15 @@ struct AxisPlan {
     int rposoff;  // offset of the R coordinate of each position
     int r[kMaxStages];
     int L[kMaxStages];
+    FastDiv fd_inner;               // divide by inner
+    FastDiv fd_nbfly[kMaxStages];   // divide by n / r
+    FastDiv fd_L[kMaxStages];       // divide by L
 };
 
 struct PlanePlan {
     AxisPlan ax[3];
     int Nk;
+    FastDiv fd_n1, fd_n2;  // position -> (q0, q1, q2) in the pointwise stage
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -155,35 +176,77 @@ struct DftGeneric {
 template <int S>
 struct Dft<7, S> : DftGeneric<7, S> {};
 
+// Composite radix R = R1*R2 entirely in registers (four-step):
+//   y[k1 + R1 k2] = sum_n2 W_R2^{n2 k2} W_R^{n2 k1} sum_n1 x[R2 n1 + n2] W_R1^{n1 k1}
+// with W_R^m = root[m * (n / R)] (conjugated for S = +1).
+template <int R1, int R2, int S>
+struct DftComposite {
+    __device__ __forceinline__ static void run(double2* v, const double2* root, int n) {
+        constexpr int R = R1 * R2;
+        const int step = n / R;
+        // phase 1, in place: v[R2 k1 + n2] <- W_R^{n2 k1} DFT_R1(v[R2 n1 + n2])_k1
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) {
+            double2 u[R1];
+#pragma unroll
+            for (int n1 = 0; n1 < R1; ++n1) u[n1] = v[R2 * n1 + n2];
+            Dft<R1, S>::run(u, root, n);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; ++k1) {
+                if (n2 * k1 == 0) {
+                    v[R2 * k1 + n2] = u[k1];
+                } else {
+                    double2 w = __ldg(&root[n2 * k1 * step]);
+                    if (S > 0) w.y = -w.y;
+                    v[R2 * k1 + n2] = cmul(u[k1], w);
+                }
+            }
+        }
+        // phase 2, in place: v[R2 k1 + k2] <- DFT_R2(v[R2 k1 + n2])_k2
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) Dft<R2, S>::run(v + R2 * k1, root, n);
+        // y[k1 + R1 k2] = v[R2 k1 + k2]: a register permutation
+        double2 y[R];
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1)
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) y[k1 + R1 * k2] = v[R2 * k1 + k2];
+#pragma unroll
+        for (int i = 0; i < R; ++i) v[i] = y[i];
+    }
+};
+template <int S>
+struct Dft<6, S> : DftComposite<2, 3, S> {};
+template <int S>
+struct Dft<9, S> : DftComposite<3, 3, S> {};
+template <int S>
+struct Dft<10, S> : DftComposite<2, 5, S> {};
+template <int S>
+struct Dft<12, S> : DftComposite<4, 3, S> {};
+
 // One radix-R stage over every line of axis `ax` of the NBUF planes that
 // start at `buf[0]`, `buf[0] + bufstride`, ...  DIF when FWD, DIT otherwise.
 template <int R, bool FWD, int NBUF>
-__device__ __forceinline__ void stage_R(double2* buf, int bufstride, int Nk, const AxisPlan& ax, int L,
+__device__ __forceinline__ void stage_R(double2* buf, int bufstride, int Nk, const AxisPlan& ax, int s,
                                         const double2* __restrict__ root) {
     constexpr int S = FWD ? -1 : +1;
     const int n = ax.n;
     const int inner = ax.inner;
+    const int L = ax.L[s];
     const int M = L * R;
     const int nbfly = n / R;
     const int tw_step = n / M;
     const int ntask = Nk / R;
+    const FastDiv fdi = ax.fd_inner, fdb = ax.fd_nbfly[s], fdl = ax.fd_L[s];
     for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
-        const int in = t % inner;
-        const int tmp = t / inner;
-        const int bfly = tmp % nbfly;
-        const int o = tmp / nbfly;
-        const int blk = bfly / L;
+        const int tmp = fdiv(t, fdi);
+        const int in = t - tmp * inner;
+        const int o = fdiv(tmp, fdb);
+        const int bfly = tmp - o * nbfly;
+        const int blk = fdiv(bfly, fdl);
         const int a = bfly - blk * L;
         const int base = o * (n * inner) + in + (blk * M + a) * inner;
         const int step = L * inner;
-        double2 tw[R];
-        tw[0] = make_double2(1.0, 0.0);
-#pragma unroll
-        for (int d = 1; d < R; ++d) {
-            double2 w = __ldg(&root[a * d * tw_step]);
-            if (!FWD) w.y = -w.y;
-            tw[d] = w;
-        }
 #pragma unroll
         for (int q = 0; q < NBUF; ++q) {
             double2* X = buf + q * bufstride;
@@ -192,11 +255,22 @@ __device__ __forceinline__ void stage_R(double2* buf, int bufstride, int Nk, con
             for (int b = 0; b < R; ++b) v[b] = X[base + b * step];
             if (FWD) {
                 Dft<R, S>::run(v, root, n);
+                if (a != 0) {
 #pragma unroll
-                for (int d = 1; d < R; ++d) v[d] = cmul(v[d], tw[d]);
+                    for (int d = 1; d < R; ++d) {
+                        double2 w = __ldg(&root[a * d * tw_step]);
+                        v[d] = cmul(v[d], w);
+                    }
+                }
             } else {
+                if (a != 0) {
 #pragma unroll
-                for (int d = 1; d < R; ++d) v[d] = cmul(v[d], tw[d]);
+                    for (int d = 1; d < R; ++d) {
+                        double2 w = __ldg(&root[a * d * tw_step]);
+                        w.y = -w.y;
+                        v[d] = cmul(v[d], w);
+                    }
+                }
                 Dft<R, S>::run(v, root, n);
             }
 #pragma unroll
@@ -209,14 +283,17 @@ template <bool FWD, int NBUF>
 __device__ __forceinline__ void run_stage(double2* buf, int bufstride, int Nk, const AxisPlan& ax, int s,
                                           const double2* __restrict__ roots) {
     const double2* root = roots + ax.rootoff;
-    const int L = ax.L[s];
     switch (ax.r[s]) {
-        case 2: stage_R<2, FWD, NBUF>(buf, bufstride, Nk, ax, L, root); break;
-        case 3: stage_R<3, FWD, NBUF>(buf, bufstride, Nk, ax, L, root); break;
-        case 4: stage_R<4, FWD, NBUF>(buf, bufstride, Nk, ax, L, root); break;
-        case 5: stage_R<5, FWD, NBUF>(buf, bufstride, Nk, ax, L, root); break;
-        case 7: stage_R<7, FWD, NBUF>(buf, bufstride, Nk, ax, L, root); break;
-        case 8: stage_R<8, FWD, NBUF>(buf, bufstride, Nk, ax, L, root); break;
+        case 2: stage_R<2, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
+        case 3: stage_R<3, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
+        case 4: stage_R<4, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
+        case 5: stage_R<5, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
+        case 6: stage_R<6, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
+        case 7: stage_R<7, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
+        case 8: stage_R<8, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
+        case 9: stage_R<9, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
+        case 10: stage_R<10, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
+        case 12: stage_R<12, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
         default: break;  // rejected on the host
     }
 }

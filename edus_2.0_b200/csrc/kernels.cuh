@@ -59,10 +59,10 @@ __global__ void __launch_bounds__(512) plane_rhs_kernel(
     const double2* r0p = rho0p + (long long)p * Nk;
     const double* wp = Wp + (long long)p * Nk;
     for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
-        const int q2 = j % n2;
-        const int t = j / n2;
-        const int q1 = t % n1;
-        const int q0 = t / n1;
+        const int t = fdiv(j, pl.fd_n2);
+        const int q2 = j - t * n2;
+        const int q0 = fdiv(t, pl.fd_n1);
+        const int q1 = t - q0 * n1;
         const double dot = F.g[0] * __ldg(&rp0[q0]) + F.g[1] * __ldg(&rp1[q1]) + F.g[2] * __ldg(&rp2[q2]);
         const double2 r = cscale(X[j], inv_nk);
         X[j] = make_double2(-dot * r.y, dot * r.x);
@@ -121,13 +121,42 @@ struct StageArgs {
     int Nk, nb, TK;
 };
 
+// Launch geometry of the commutator kernel (shared by every caller).
+// Each thread computes 2x2 output tiles of one k point and holds at most two
+// tiles in registers, so TK (k points per CTA) is the largest power of two
+// with TK * tiles <= 2 * threads; threads is 256, or 512 when even TK = 1
+// needs more.  Shared memory: H and rho tiles [TK][nbp][nbp+1] (nbp = nb
+// rounded up to even; the odd row pitch spreads rows over the banks) and the
+// Hartree shift [nb].  The commutator result is staged over the H tiles.
+struct CommGeom {
+    int TK, threads, nbp, ld;
+    size_t smem;
+};
+
+__host__ __device__ inline CommGeom comm_geometry(int nb) {
+    CommGeom g;
+    g.nbp = (nb + 1) & ~1;
+    g.ld = g.nbp + 1;
+    const int ntile = (g.nbp / 2) * (g.nbp / 2);
+    int tk = 64;
+    while (tk > 1 && tk * ntile > 512) tk /= 2;
+    while (tk > 1 && (2 * (size_t)tk * g.nbp * g.ld + nb) * 16 > 100 * 1024) tk /= 2;
+    g.TK = tk;
+    g.threads = (tk * ntile > 512) ? 512 : 256;
+    g.smem = (2 * (size_t)tk * g.nbp * g.ld + nb) * 16;
+    return g;
+}
+
 template <int MODE, bool COUL>
-__global__ void __launch_bounds__(256) commutator_kernel(StageArgs a) {
+__global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
     extern __shared__ double2 sm[];
     const int nb = a.nb, P = nb * nb, TK = a.TK, Nk = a.Nk;
-    double2* Hs = sm;            // [P][TK]
-    double2* Rs = sm + P * TK;   // [P][TK]
-    double2* hh = Rs + P * TK;   // [nb] Hartree shift
+    const int nbp = (nb + 1) & ~1, ld = nbp + 1;
+    const int tile_stride = nbp * ld;
+    double2* Hs = sm;                        // [TK][nbp][ld]
+    double2* Rs = sm + TK * tile_stride;     // [TK][nbp][ld]
+    double2* hh = Rs + TK * tile_stride;     // [nb] Hartree shift
+    double2* Cs = sm;                        // [P][TK], over Hs once the products are done
     const int b = blockIdx.y;
     const int k0 = blockIdx.x * TK;
     const long long boff = (long long)b * a.bstride;
@@ -149,6 +178,7 @@ __global__ void __launch_bounds__(256) commutator_kernel(StageArgs a) {
         const int p = idx / TK, kk = idx - (idx / TK) * TK;
         const int k = k0 + kk;
         double2 h = make_double2(0.0, 0.0), r = make_double2(0.0, 0.0);
+        const int i = p / nb, j = p - (p / nb) * nb;
         if (k < Nk) {
             const long long e = (long long)p * Nk + k;
             r = __ldg(&a.rho[boff + e]);
@@ -158,38 +188,85 @@ __global__ void __launch_bounds__(256) commutator_kernel(StageArgs a) {
             if (e2) { double2 x = __ldg(&a.xi[2][e]); h.x += F.E[2] * x.x; h.y += F.E[2] * x.y; }
             if (COUL) {
                 h = cadd(h, __ldg(&a.Hee[boff + e]));
-                const int n = p / nb;
-                if (p == n * nb + n) h = cadd(h, hh[n]);
+                if (i == j) h = cadd(h, hh[i]);
             }
         }
-        Hs[idx] = h;
-        Rs[idx] = r;
+        const int o = kk * tile_stride + i * ld + j;
+        Hs[o] = h;
+        Rs[o] = r;
+    }
+    __syncthreads();
+    // C = H rho - rho H on 2x2 tiles (rows i0, i0+1; columns j0, j0+1) of one
+    // k point: per l, 8 shared loads feed 8 complex multiply-adds.
+    const int half = nbp / 2;
+    const int ntile = half * half;
+    const int ntask = TK * ntile;
+    double2 acc[2][4];
+#pragma unroll
+    for (int t = 0; t < 2; ++t)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[t][q] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const int task = threadIdx.x + t * blockDim.x;
+        if (task < ntask) {
+            const int kk = task / ntile, tt = task - (task / ntile) * ntile;
+            const int i0 = 2 * (tt / half), j0 = 2 * (tt - (tt / half) * half);
+            const double2* H = Hs + kk * tile_stride;
+            const double2* R = Rs + kk * tile_stride;
+            double2 c00 = make_double2(0.0, 0.0), c01 = c00, c10 = c00, c11 = c00;
+            for (int l = 0; l < nb; ++l) {
+                const double2 h0 = H[i0 * ld + l], h1 = H[(i0 + 1) * ld + l];
+                const double2 r0 = R[l * ld + j0], r1 = R[l * ld + j0 + 1];
+                c00.x = fma(h0.x, r0.x, fma(-h0.y, r0.y, c00.x));
+                c00.y = fma(h0.x, r0.y, fma(h0.y, r0.x, c00.y));
+                c01.x = fma(h0.x, r1.x, fma(-h0.y, r1.y, c01.x));
+                c01.y = fma(h0.x, r1.y, fma(h0.y, r1.x, c01.y));
+                c10.x = fma(h1.x, r0.x, fma(-h1.y, r0.y, c10.x));
+                c10.y = fma(h1.x, r0.y, fma(h1.y, r0.x, c10.y));
+                c11.x = fma(h1.x, r1.x, fma(-h1.y, r1.y, c11.x));
+                c11.y = fma(h1.x, r1.y, fma(h1.y, r1.x, c11.y));
+                const double2 q0 = R[i0 * ld + l], q1 = R[(i0 + 1) * ld + l];
+                const double2 g0 = H[l * ld + j0], g1 = H[l * ld + j0 + 1];
+                c00.x = fma(-q0.x, g0.x, fma(q0.y, g0.y, c00.x));
+                c00.y = fma(-q0.x, g0.y, fma(-q0.y, g0.x, c00.y));
+                c01.x = fma(-q0.x, g1.x, fma(q0.y, g1.y, c01.x));
+                c01.y = fma(-q0.x, g1.y, fma(-q0.y, g1.x, c01.y));
+                c10.x = fma(-q1.x, g0.x, fma(q1.y, g0.y, c10.x));
+                c10.y = fma(-q1.x, g0.y, fma(-q1.y, g0.x, c10.y));
+                c11.x = fma(-q1.x, g1.x, fma(q1.y, g1.y, c11.x));
+                c11.y = fma(-q1.x, g1.y, fma(-q1.y, g1.x, c11.y));
+            }
+            acc[t][0] = c00;
+            acc[t][1] = c01;
+            acc[t][2] = c10;
+            acc[t][3] = c11;
+        }
+    }
+    __syncthreads();  // every tile read is done: Cs may overwrite Hs
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const int task = threadIdx.x + t * blockDim.x;
+        if (task < ntask) {
+            const int kk = task / ntile, tt = task - (task / ntile) * ntile;
+            const int i0 = 2 * (tt / half), j0 = 2 * (tt - (tt / half) * half);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int i = i0 + (q >> 1), j = j0 + (q & 1);
+                if (i < nb && j < nb) Cs[(i * nb + j) * TK + kk] = acc[t][q];
+            }
+        }
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < P * TK; idx += blockDim.x) {
         const int p = idx / TK, kk = idx - (idx / TK) * TK;
         const int k = k0 + kk;
         if (k >= Nk) continue;
-        const int i = p / nb, j = p - (p / nb) * nb;
-        double cr = 0.0, ci = 0.0;  // C = H rho - rho H
-        for (int l = 0; l < nb; ++l) {
-            const double2 hil = Hs[(i * nb + l) * TK + kk];
-            const double2 rlj = Rs[(l * nb + j) * TK + kk];
-            const double2 ril = Rs[(i * nb + l) * TK + kk];
-            const double2 hlj = Hs[(l * nb + j) * TK + kk];
-            cr = fma(hil.x, rlj.x, cr);
-            cr = fma(-hil.y, rlj.y, cr);
-            ci = fma(hil.x, rlj.y, ci);
-            ci = fma(hil.y, rlj.x, ci);
-            cr = fma(-ril.x, hlj.x, cr);
-            cr = fma(ril.y, hlj.y, cr);
-            ci = fma(-ril.x, hlj.y, ci);
-            ci = fma(-ril.y, hlj.x, ci);
-        }
+        const double2 c = Cs[idx];
         const long long e = boff + (long long)p * Nk + k;
         const double2 g = __ldg(&a.G[e]);
         // f = G - i C
-        const double2 f = make_double2(g.x + ci, g.y - cr);
+        const double2 f = make_double2(g.x + c.y, g.y - c.x);
         if (MODE == MODE_RHS) {
             a.out[e] = f;
         } else if (MODE == MODE_RK1) {

@@ -69,6 +69,10 @@ CASES = [
     ("g7", (7, 14, 1), 2, 2, True),
     ("g50", (50, 50, 1), 2, 2, True),
     ("g64", (64, 8, 1), 3, 2, False),
+    ("g36", (36, 12, 1), 2, 2, True),     # radix 12 then 3, and radix 12 alone
+    ("g3d_6x9x4", (6, 9, 4), 2, 3, False),
+    ("g120", (120, 120, 1), 2, 2, False),  # 230 KB plane in shared memory; radices 12 and 10
+    ("g96", (96, 20, 1), 5, 2, True),      # odd nb: padded 2x2 commutator tiles
 ]
 
 
