@@ -41,6 +41,7 @@ struct edus_handle {
     double A[9] = {0};  // lattice, row-major, vectors in columns
     PlanePlan plan{};
     int smem_plane = 0, smem_comm = 0, TK = 4, comm_threads = 256;
+    bool comm_mma = false;
     unsigned long long launches = 0;
     size_t dev_bytes = 0;
     std::vector<std::vector<edus_laser>> lasers;
@@ -199,10 +200,17 @@ int launch_comm_mode(edus_handle* h, const StageArgs& a, int nbatch) {
     dim3 grid((h->Nk + h->TK - 1) / h->TK, nbatch);
     cudaEvent_t e0;
     prof_begin(h, &e0);
-    if (h->d.coulomb)
-        commutator_kernel<MODE, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
-    else
-        commutator_kernel<MODE, false><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
+    if (h->comm_mma) {
+        if (h->d.coulomb)
+            commutator_mma_kernel<MODE, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
+        else
+            commutator_mma_kernel<MODE, false><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
+    } else {
+        if (h->d.coulomb)
+            commutator_kernel<MODE, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
+        else
+            commutator_kernel<MODE, false><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
+    }
     h->launches++;
     CU(h, cudaGetLastError());
     prof_end(h, 1, e0);
@@ -304,17 +312,20 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
                          "k grid of " + std::to_string(h->Nk) + " points does not fit one plane" +
                              (d.coulomb ? " pair" : "") + " in shared memory (" + std::to_string(dev_smem) + " B)"));
     h->smem_plane = (int)plane_bytes;
-    const CommGeom cg = comm_geometry(h->nb);
-    h->TK = cg.TK;
-    h->comm_threads = cg.threads;
-    h->smem_comm = (int)cg.smem;
+    const CommLaunch cl = comm_launch(h->nb);
+    h->comm_mma = cl.mma;
+    h->TK = cl.TK;
+    h->comm_threads = cl.threads;
+    h->smem_comm = (int)cl.smem;
     if (h->smem_comm > dev_smem) return bail(fail(h, EDUS_ERR_UNSUPPORTED, "too many bands for the commutator tile"));
     int rc;
     if ((rc = set_smem(h, plane_rhs_kernel<true>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_rhs_kernel<false>, h->smem_plane))) return bail(rc);
 #define SETC(M)                                                                                   \
     if ((rc = set_smem(h, commutator_kernel<M, true>, h->smem_comm))) return bail(rc);           \
-    if ((rc = set_smem(h, commutator_kernel<M, false>, h->smem_comm))) return bail(rc);
+    if ((rc = set_smem(h, commutator_kernel<M, false>, h->smem_comm))) return bail(rc);          \
+    if ((rc = set_smem(h, commutator_mma_kernel<M, true>, h->smem_comm))) return bail(rc);       \
+    if ((rc = set_smem(h, commutator_mma_kernel<M, false>, h->smem_comm))) return bail(rc);
     SETC(MODE_RHS) SETC(MODE_RK1) SETC(MODE_RK2) SETC(MODE_RK3) SETC(MODE_RK4) SETC(MODE_AB)
 #undef SETC
 

@@ -153,7 +153,7 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
                                                std::to_string((size_t)EDUS_NOALLOC_SCRATCH_BYTES) +
                                                " (use edus_create/edus_rhs)");
     const size_t plane_smem = (size_t)Nk * sizeof(double2) * (coulomb ? 2 : 1);
-    const CommGeom cgeo = comm_geometry(nb);
+    const CommLaunch cgeo = comm_launch(nb);
     const int tk = cgeo.TK;
     const size_t comm_smem = cgeo.smem;
 
@@ -181,7 +181,9 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
             if ((e = cudaFuncSetAttribute(plane_rhs_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
                 (e = cudaFuncSetAttribute(plane_rhs_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
                 (e = cudaFuncSetAttribute(commutator_kernel<MODE_RHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
-                (e = cudaFuncSetAttribute(commutator_kernel<MODE_RHS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess)
+                (e = cudaFuncSetAttribute(commutator_kernel<MODE_RHS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
+                (e = cudaFuncSetAttribute(commutator_mma_kernel<MODE_RHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
+                (e = cudaFuncSetAttribute(commutator_mma_kernel<MODE_RHS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess)
                 return nfail(EDUS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
             g_smem_set[dev] = lim;
         }
@@ -257,10 +259,17 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
     a.nb = nb;
     a.TK = tk;
     dim3 cg((Nk + tk - 1) / tk, 1);
-    if (coulomb)
-        commutator_kernel<MODE_RHS, true><<<cg, cgeo.threads, comm_smem, stream>>>(a);
-    else
-        commutator_kernel<MODE_RHS, false><<<cg, cgeo.threads, comm_smem, stream>>>(a);
+    if (cgeo.mma) {
+        if (coulomb)
+            commutator_mma_kernel<MODE_RHS, true><<<cg, cgeo.threads, comm_smem, stream>>>(a);
+        else
+            commutator_mma_kernel<MODE_RHS, false><<<cg, cgeo.threads, comm_smem, stream>>>(a);
+    } else {
+        if (coulomb)
+            commutator_kernel<MODE_RHS, true><<<cg, cgeo.threads, comm_smem, stream>>>(a);
+        else
+            commutator_kernel<MODE_RHS, false><<<cg, cgeo.threads, comm_smem, stream>>>(a);
+    }
     NA_CU(cudaGetLastError());
     dim3 tg2((P + 31) / 32, (Nk + 31) / 32);
     transpose_pk_to_kp<<<tg2, tb, 0, stream>>>(out_pk, (double2*)out_k, Nk, P);

@@ -295,6 +295,210 @@ __global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Tensor-core commutator for nb >= 12: the same contract as commutator_kernel,
+// with C = H rho - rho H done by FP64 warp MMAs (mma.sync m8n8k4, 8x8 output
+// tiles, K steps of 4).  A complex product is four real products:
+//   Re(A B) = Ar Br - Ai Bi,  Im(A B) = Ar Bi + Ai Br,
+// so each (tile, K step) issues 8 MMAs (4 for H rho, 4 for -rho H).
+// Shared memory per k point: Hr, Hi, Rr, Ri as [nbp][pitch] doubles, nbp = nb
+// rounded up to 8 and zero-padded, pitch = nbp + 4 (the fragment rows of a
+// half-warp then land on distinct bank groups).  TK k points per CTA, 8 warps,
+// 8/TK warps per k point; the result is staged as [p][TK] over the tiles.
+struct MmaGeom {
+    int TK, nbp, pitch, tiles, warps_per_k;
+    size_t smem;
+};
+
+__host__ __device__ inline MmaGeom mma_geometry(int nb) {
+    MmaGeom g;
+    g.nbp = (nb + 7) & ~7;
+    g.pitch = g.nbp + 4;
+    g.tiles = g.nbp / 8;
+    const size_t per_k = 4 * (size_t)g.nbp * g.pitch * 8;
+    const int ntile = g.tiles * g.tiles;
+    g.TK = 1;
+    if (4 * per_k <= 100 * 1024 && (ntile + 1) / 2 <= 8) g.TK = 4;
+    else if (2 * per_k <= 160 * 1024 && (ntile + 3) / 4 <= 8) g.TK = 2;
+    g.warps_per_k = 8 / g.TK;
+    g.smem = g.TK * per_k + (size_t)nb * 16;
+    return g;
+}
+
+// Which commutator kernel a band count uses (the tensor-core one from 12
+// bands up) and its launch geometry.
+struct CommLaunch {
+    bool mma;
+    int TK, threads;
+    size_t smem;
+};
+inline CommLaunch comm_launch(int nb) {
+    CommLaunch c;
+    c.mma = nb >= 12;
+    if (c.mma) {
+        const MmaGeom g = mma_geometry(nb);
+        c.TK = g.TK;
+        c.threads = 256;
+        c.smem = g.smem;
+    } else {
+        const CommGeom g = comm_geometry(nb);
+        c.TK = g.TK;
+        c.threads = g.threads;
+        c.smem = g.smem;
+    }
+    return c;
+}
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <int MODE, bool COUL>
+__global__ void __launch_bounds__(256) commutator_mma_kernel(StageArgs a) {
+    extern __shared__ double smd[];
+    const int nb = a.nb, P = nb * nb, Nk = a.Nk;
+    const MmaGeom g = mma_geometry(nb);
+    const int TK = g.TK, nbp = g.nbp, pitch = g.pitch;
+    const int mat = nbp * pitch;  // doubles per matrix
+    double* tiles = smd;          // [TK][4][nbp][pitch]: Hr, Hi, Rr, Ri
+    double2* hh = (double2*)(smd + (size_t)TK * 4 * mat);
+    double2* Cs = (double2*)smd;  // [P][TK] after the products
+    const int b = blockIdx.y;
+    const int k0 = blockIdx.x * TK;
+    const long long boff = (long long)b * a.bstride;
+    const StageField F = a.field[b];
+    for (int i = threadIdx.x; i < TK * 4 * mat; i += blockDim.x) tiles[i] = 0.0;
+    if (COUL) {
+        for (int n = threadIdx.x; n < nb; n += blockDim.x) {
+            double2 s = make_double2(0.0, 0.0);
+            for (int m = 0; m < nb; ++m) {
+                const double2 d0 = a.diag0[b * nb + m];
+                const double2 r0 = a.rho0diag[m];
+                s = cadd(s, cmul(a.hartree[n * nb + m], csub(d0, r0)));
+            }
+            hh[n] = s;
+        }
+    }
+    __syncthreads();
+    const bool e0 = F.E[0] != 0.0, e1 = F.E[1] != 0.0, e2 = F.E[2] != 0.0;
+    for (int idx = threadIdx.x; idx < P * TK; idx += blockDim.x) {
+        const int p = idx / TK, kk = idx - (idx / TK) * TK;
+        const int k = k0 + kk;
+        if (k >= Nk) continue;
+        const int i = p / nb, j = p - (p / nb) * nb;
+        const long long e = (long long)p * Nk + k;
+        const double2 r = __ldg(&a.rho[boff + e]);
+        double2 h = __ldg(&a.H0[e]);
+        if (e0) { double2 x = __ldg(&a.xi[0][e]); h.x += F.E[0] * x.x; h.y += F.E[0] * x.y; }
+        if (e1) { double2 x = __ldg(&a.xi[1][e]); h.x += F.E[1] * x.x; h.y += F.E[1] * x.y; }
+        if (e2) { double2 x = __ldg(&a.xi[2][e]); h.x += F.E[2] * x.x; h.y += F.E[2] * x.y; }
+        if (COUL) {
+            h = cadd(h, __ldg(&a.Hee[boff + e]));
+            if (i == j) h = cadd(h, hh[i]);
+        }
+        double* T = tiles + (size_t)kk * 4 * mat + i * pitch + j;
+        T[0] = h.x;
+        T[mat] = h.y;
+        T[2 * mat] = r.x;
+        T[3 * mat] = r.y;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kk = warp / g.warps_per_k, part = warp - kk * g.warps_per_k;
+    const int ntile = g.tiles * g.tiles;
+    const int per = (ntile + g.warps_per_k - 1) / g.warps_per_k;
+    const int t0 = part * per, t1 = min(ntile, t0 + per);
+    constexpr int MAXT = 8;  // tiles per warp (nb <= 64)
+    double cr[MAXT][2], ci[MAXT][2];
+#pragma unroll
+    for (int t = 0; t < MAXT; ++t) cr[t][0] = cr[t][1] = ci[t][0] = ci[t][1] = 0.0;
+    const double* Hr = tiles + (size_t)kk * 4 * mat;
+    const double* Hi = Hr + mat;
+    const double* Rr = Hr + 2 * mat;
+    const double* Ri = Hr + 3 * mat;
+    const int ar = lane >> 2, ac = lane & 3;  // A fragment (row, col); B fragment (row = ac, col = ar)
+    if (kk < TK && k0 + kk < Nk) {
+        for (int ks = 0; ks < nbp / 4; ++ks) {
+            const int kc = ks * 4 + ac;
+#pragma unroll
+            for (int t = 0; t < MAXT; ++t) {
+                const int tt = t0 + t;
+                if (tt < t1) {
+                    const int ti = tt / g.tiles, tj = tt - (tt / g.tiles) * g.tiles;
+                    const int arow = ti * 8 + ar;   // output row of the A fragment
+                    const int bcol = tj * 8 + ar;   // output column of the B fragment
+                    // H rho
+                    const double hr = Hr[arow * pitch + kc], hi = Hi[arow * pitch + kc];
+                    const double rr = Rr[kc * pitch + bcol], ri = Ri[kc * pitch + bcol];
+                    dmma(cr[t][0], cr[t][1], hr, rr);
+                    dmma(cr[t][0], cr[t][1], -hi, ri);
+                    dmma(ci[t][0], ci[t][1], hr, ri);
+                    dmma(ci[t][0], ci[t][1], hi, rr);
+                    // - rho H
+                    const double qr = Rr[arow * pitch + kc], qi = Ri[arow * pitch + kc];
+                    const double gr = Hr[kc * pitch + bcol], gi = Hi[kc * pitch + bcol];
+                    dmma(cr[t][0], cr[t][1], -qr, gr);
+                    dmma(cr[t][0], cr[t][1], qi, gi);
+                    dmma(ci[t][0], ci[t][1], -qr, gi);
+                    dmma(ci[t][0], ci[t][1], -qi, gr);
+                }
+            }
+        }
+    }
+    __syncthreads();  // all fragments read: Cs may overwrite the tiles
+    if (kk < TK) {
+#pragma unroll
+        for (int t = 0; t < MAXT; ++t) {
+            const int tt = t0 + t;
+            if (tt < t1) {
+                const int ti = tt / g.tiles, tj = tt - (tt / g.tiles) * g.tiles;
+                const int row = ti * 8 + ar;
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int col = tj * 8 + ac * 2 + q;
+                    if (row < nb && col < nb) Cs[(row * nb + col) * TK + kk] = make_double2(cr[t][q], ci[t][q]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < P * TK; idx += blockDim.x) {
+        const int p = idx / TK, kq = idx - (idx / TK) * TK;
+        const int k = k0 + kq;
+        if (k >= Nk) continue;
+        const double2 c = Cs[idx];
+        const long long e = boff + (long long)p * Nk + k;
+        const double2 gg = __ldg(&a.G[e]);
+        const double2 f = make_double2(gg.x + c.y, gg.y - c.x);
+        if (MODE == MODE_RHS) {
+            a.out[e] = f;
+        } else if (MODE == MODE_RK1) {
+            const double2 y = a.y[e];
+            a.aux[e] = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
+            a.acc[e] = make_double2(y.x + a.c[1] * f.x, y.y + a.c[1] * f.y);
+        } else if (MODE == MODE_RK2 || MODE == MODE_RK3) {
+            const double2 y = a.y[e];
+            const double2 ac2 = a.acc[e];
+            a.aux[e] = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
+            a.acc[e] = make_double2(ac2.x + a.c[1] * f.x, ac2.y + a.c[1] * f.y);
+        } else if (MODE == MODE_RK4) {
+            const double2 ac2 = a.acc[e];
+            a.y[e] = make_double2(ac2.x + a.c[0] * f.x, ac2.y + a.c[0] * f.y);
+        } else if (MODE == MODE_AB) {
+            a.hist[0][e] = f;
+            double2 y = a.y[e];
+            y = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
+            for (int q = 1; q < a.order; ++q) {
+                const double2 fq = a.hist[q][e];
+                y = make_double2(y.x + a.c[q] * fq.x, y.y + a.c[q] * fq.y);
+            }
+            a.y[e] = y;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Layout transposes between the reference's [k][p] and the plane-major [p][k].
 __global__ void transpose_kp_to_pk(const double2* __restrict__ src, double2* __restrict__ dst, int Nk, int P) {
     __shared__ double2 tile[32][33];

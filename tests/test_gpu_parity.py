@@ -73,6 +73,11 @@ CASES = [
     ("g3d_6x9x4", (6, 9, 4), 2, 3, False),
     ("g120", (120, 120, 1), 2, 2, False),  # 230 KB plane in shared memory; radices 12 and 10
     ("g96", (96, 20, 1), 5, 2, True),      # odd nb: padded 2x2 commutator tiles
+    # tensor-core (FP64 MMA) commutator from 12 bands: padded 8x8 tiles, TK 4 / 2
+    ("mma12", (12, 8, 1), 12, 2, True),
+    ("mma14", (10, 6, 1), 14, 2, False),
+    ("mma17", (8, 6, 1), 17, 2, True),
+    ("mma33", (6, 4, 1), 33, 2, True),
 ]
 
 
@@ -106,6 +111,19 @@ def test_steps_parity(pkg, po, tmp_path, solver, order, coulomb):
         assert np.abs(ref).max() < 10 * n0  # a bounded (physical) trajectory
         assert rel(s.get_state(), ref) < TOL
         assert s.time == pytest.approx(o.time, rel=0, abs=1e-12)
+
+
+@pytest.mark.parametrize("solver,order", [("RK", 4), ("AB", 4)])
+def test_steps_parity_mma(pkg, po, tmp_path, solver, order):
+    inp = model_input(pkg, tmp_path, f"stm_{solver}{order}", (8, 9, 1), nb=13, coulomb=True, solver=solver,
+                      order=order, dt=0.01)
+    cfg, o, s = make_pair(pkg, po, inp, batch=2)
+    for chunk in (1, 4, 10):
+        s.step(chunk)
+        o.step(chunk)
+        ref = o.get("rho")
+        assert rel(s.get_state(0), ref) < TOL
+        assert rel(s.get_state(1), ref) < TOL
 
 
 def test_batch_equals_separate_solves(pkg, po, tmp_path):
