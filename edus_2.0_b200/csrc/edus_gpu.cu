@@ -42,6 +42,9 @@ struct edus_handle {
     PlanePlan plan{};
     int smem_plane = 0, smem_comm = 0, TK = 4, comm_threads = 256;
     bool comm_mma = false;
+    PlaneLaunch plane_cfg{0, 512, false};
+    int plane_grid = 0;            // persistent plane kernel: CTAs per launch
+    double2* plane_scratch = nullptr;  // [plane_grid][Nk]: rho(R) between the two inverse transforms
     unsigned long long launches = 0;
     size_t dev_bytes = 0;
     std::vector<std::vector<edus_laser>> lasers;
@@ -176,19 +179,45 @@ void prof_resolve(edus_handle* h) {
     h->prof_pending.clear();
 }
 
+template <bool COUL, int MASK, int MAXT>
+void launch_plane_variant(edus_handle* h, dim3 grid, const double2* in, long long in_bstride, double2* G,
+                          double2* Hee, long long out_bstride, const StageField* field) {
+    plane_rhs_kernel<COUL, MASK, MAXT><<<grid, h->plane_cfg.threads, h->smem_plane, h->stream>>>(
+        in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
+        1.0 / h->Nk);
+}
+
+template <bool COUL, int MASK, int MAXT>
+void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long long in_bstride, double2* G,
+                          double2* Hee, long long out_bstride, const StageField* field) {
+    const int grid = std::min(nplanes, h->plane_grid);
+    plane_rhs_persist_kernel<COUL, MASK, MAXT><<<grid, h->plane_cfg.threads, h->Nk * sizeof(double2), h->stream>>>(
+        in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
+        1.0 / h->Nk, h->plane_scratch, nplanes);
+}
+
 int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double2* G, double2* Hee,
                  long long out_bstride, const StageField* field, int nbatch) {
     dim3 grid(h->P, nbatch);
     cudaEvent_t e0;
     prof_begin(h, &e0);
-    if (h->d.coulomb)
-        plane_rhs_kernel<true><<<grid, 512, h->smem_plane, h->stream>>>(in, in_bstride, G, Hee, out_bstride, h->rho0p,
-                                                                         h->Wp, h->diag0, field, h->roots, h->rpos,
-                                                                         h->plan, h->nb, 1.0 / h->Nk);
-    else
-        plane_rhs_kernel<false><<<grid, 512, h->smem_plane, h->stream>>>(in, in_bstride, G, Hee, out_bstride, h->rho0p,
-                                                                          h->Wp, h->diag0, field, h->roots, h->rpos,
-                                                                          h->plan, h->nb, 1.0 / h->Nk);
+    const bool c = h->d.coulomb != 0;
+    if (h->plane_cfg.persist) {
+        const int np = h->P * nbatch;
+        if (h->plane_cfg.variant == 1) {
+            if (c) launch_plane_persist<true, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field);
+            else launch_plane_persist<false, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field);
+        } else {
+            if (c) launch_plane_persist<true, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field);
+            else launch_plane_persist<false, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field);
+        }
+    } else if (h->plane_cfg.variant == 1) {
+        if (c) launch_plane_variant<true, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field);
+        else launch_plane_variant<false, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field);
+    } else {
+        if (c) launch_plane_variant<true, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field);
+        else launch_plane_variant<false, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field);
+    }
     h->launches++;
     CU(h, cudaGetLastError());
     prof_end(h, 0, e0);
@@ -319,8 +348,23 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     h->smem_comm = (int)cl.smem;
     if (h->smem_comm > dev_smem) return bail(fail(h, EDUS_ERR_UNSUPPORTED, "too many bands for the commutator tile"));
     int rc;
-    if ((rc = set_smem(h, plane_rhs_kernel<true>, h->smem_plane))) return bail(rc);
-    if ((rc = set_smem(h, plane_rhs_kernel<false>, h->smem_plane))) return bail(rc);
+    h->plane_cfg = plane_launch(h->plan);
+    {
+        int nsm = 0;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d.device);
+        h->plane_grid = 2 * std::max(nsm, 1);
+    }
+    {
+        const int ps = h->Nk * (int)sizeof(double2);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadix89, 384>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadix89, 384>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadixAll, 256>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadixAll, 256>, ps))) return bail(rc);
+    }
+    if ((rc = set_smem(h, plane_rhs_kernel<true, kRadixAll, 512>, h->smem_plane))) return bail(rc);
+    if ((rc = set_smem(h, plane_rhs_kernel<false, kRadixAll, 512>, h->smem_plane))) return bail(rc);
+    if ((rc = set_smem(h, plane_rhs_kernel<true, kRadix89, 768>, h->smem_plane))) return bail(rc);
+    if ((rc = set_smem(h, plane_rhs_kernel<false, kRadix89, 768>, h->smem_plane))) return bail(rc);
 #define SETC(M)                                                                                   \
     if ((rc = set_smem(h, commutator_kernel<M, true>, h->smem_comm))) return bail(rc);           \
     if ((rc = set_smem(h, commutator_kernel<M, false>, h->smem_comm))) return bail(rc);          \
@@ -367,6 +411,7 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     TRY_ALLOC(h->roots, roots.size() * sizeof(double2));
     TRY_ALLOC(h->rpos, rpos.size() * sizeof(double));
     TRY_ALLOC(h->field, (size_t)h->chunk * 4 * h->B * sizeof(StageField));
+    if (h->plane_cfg.persist && d.coulomb) TRY_ALLOC(h->plane_scratch, (size_t)h->plane_grid * h->Nk * sizeof(double2));
     TRY_ALLOC(h->popbuf, h->nb * sizeof(double));
     TRY_ALLOC(h->flag, sizeof(int));
 #undef TRY_ALLOC

@@ -178,8 +178,8 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
         }
         if (g_smem_set[dev] < dev_smem) {
             const int lim = dev_smem;
-            if ((e = cudaFuncSetAttribute(plane_rhs_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
-                (e = cudaFuncSetAttribute(plane_rhs_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
+            if ((e = cudaFuncSetAttribute(plane_rhs_kernel<true, kRadixAll, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
+                (e = cudaFuncSetAttribute(plane_rhs_kernel<false, kRadixAll, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
                 (e = cudaFuncSetAttribute(commutator_kernel<MODE_RHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
                 (e = cudaFuncSetAttribute(commutator_kernel<MODE_RHS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
                 (e = cudaFuncSetAttribute(commutator_mma_kernel<MODE_RHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) != cudaSuccess ||
@@ -237,11 +237,13 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
     NA_CU(cudaGetLastError());
     dim3 pg(P, 1);
     if (coulomb)
-        plane_rhs_kernel<true><<<pg, 512, plane_smem, stream>>>(rho_pk, 0, G, Hee, 0, r0p, Wp, diag0, d_field, d_roots,
-                                                                 d_rpos, plan, nb, 1.0 / Nk);
+        plane_rhs_kernel<true, kRadixAll, 512><<<pg, 512, plane_smem, stream>>>(rho_pk, 0, G, Hee, 0, r0p, Wp, diag0,
+                                                                                 d_field, d_roots, d_rpos, plan, nb,
+                                                                                 1.0 / Nk);
     else
-        plane_rhs_kernel<false><<<pg, 512, plane_smem, stream>>>(rho_pk, 0, G, Hee, 0, r0p, Wp, diag0, d_field, d_roots,
-                                                                  d_rpos, plan, nb, 1.0 / Nk);
+        plane_rhs_kernel<false, kRadixAll, 512><<<pg, 512, plane_smem, stream>>>(rho_pk, 0, G, Hee, 0, r0p, Wp, diag0,
+                                                                                  d_field, d_roots, d_rpos, plan, nb,
+                                                                                  1.0 / Nk);
     NA_CU(cudaGetLastError());
     StageArgs a{};
     a.rho = rho_pk;

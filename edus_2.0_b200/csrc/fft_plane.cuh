@@ -279,48 +279,58 @@ __device__ __forceinline__ void stage_R(double2* buf, int bufstride, int Nk, con
     }
 }
 
-template <bool FWD, int NBUF>
+// Radix sets a plane kernel may be specialised for (bit r set = radix r).
+constexpr int kRadixAll = (1 << 2) | (1 << 3) | (1 << 4) | (1 << 5) | (1 << 6) | (1 << 7) | (1 << 8) | (1 << 9) |
+                          (1 << 10) | (1 << 12);
+constexpr int kRadix89 = (1 << 8) | (1 << 9);
+
+template <bool FWD, int NBUF, int MASK>
 __device__ __forceinline__ void run_stage(double2* buf, int bufstride, int Nk, const AxisPlan& ax, int s,
                                           const double2* __restrict__ roots) {
     const double2* root = roots + ax.rootoff;
     switch (ax.r[s]) {
-        case 2: stage_R<2, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
-        case 3: stage_R<3, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
-        case 4: stage_R<4, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
-        case 5: stage_R<5, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
-        case 6: stage_R<6, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
-        case 7: stage_R<7, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
-        case 8: stage_R<8, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
-        case 9: stage_R<9, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
-        case 10: stage_R<10, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
-        case 12: stage_R<12, FWD, NBUF>(buf, bufstride, Nk, ax, s, root); break;
-        default: break;  // rejected on the host
+#define EDUS_STAGE_CASE(R)                                                                          \
+    case R:                                                                                         \
+        if constexpr ((MASK >> R) & 1) stage_R<R, FWD, NBUF>(buf, bufstride, Nk, ax, s, root);   \
+        break;
+        EDUS_STAGE_CASE(2)
+        EDUS_STAGE_CASE(3)
+        EDUS_STAGE_CASE(4)
+        EDUS_STAGE_CASE(5)
+        EDUS_STAGE_CASE(6)
+        EDUS_STAGE_CASE(7)
+        EDUS_STAGE_CASE(8)
+        EDUS_STAGE_CASE(9)
+        EDUS_STAGE_CASE(10)
+        EDUS_STAGE_CASE(12)
+#undef EDUS_STAGE_CASE
+        default: break;  // the host never selects a kernel lacking a radix of its plan
     }
 }
 
 // Forward (k -> R, unnormalised sign -1) transform of the plane(s) in place.
-template <int NBUF>
+template <int NBUF, int MASK>
 __device__ void plane_forward(double2* buf, int bufstride, const PlanePlan& pl, const double2* __restrict__ roots) {
 #pragma unroll 1
     for (int d = 0; d < 3; ++d) {
         const AxisPlan& ax = pl.ax[d];
 #pragma unroll 1
         for (int s = 0; s < ax.nst; ++s) {
-            run_stage<true, NBUF>(buf, bufstride, pl.Nk, ax, s, roots);
+            run_stage<true, NBUF, MASK>(buf, bufstride, pl.Nk, ax, s, roots);
             __syncthreads();
         }
     }
 }
 
 // Inverse (R -> k, unnormalised sign +1) transform, exact reverse of plane_forward.
-template <int NBUF>
+template <int NBUF, int MASK>
 __device__ void plane_inverse(double2* buf, int bufstride, const PlanePlan& pl, const double2* __restrict__ roots) {
 #pragma unroll 1
     for (int d = 2; d >= 0; --d) {
         const AxisPlan& ax = pl.ax[d];
 #pragma unroll 1
         for (int s = ax.nst - 1; s >= 0; --s) {
-            run_stage<false, NBUF>(buf, bufstride, pl.Nk, ax, s, roots);
+            run_stage<false, NBUF, MASK>(buf, bufstride, pl.Nk, ax, s, roots);
             __syncthreads();
         }
     }

@@ -31,8 +31,8 @@ struct StageField {
 // and rho_nn(R=0) of diagonal planes is written to diag0 for the Hartree term.
 // Reference: Functional_SourceTerm.hpp:15-50, kGradient_definitions.hpp:35-40,
 // Coulomb.cpp:150-171, fftPair.cpp:89-107.
-template <bool COUL>
-__global__ void __launch_bounds__(512) plane_rhs_kernel(
+template <bool COUL, int MASK, int MAXT>
+__global__ void __launch_bounds__(MAXT) plane_rhs_kernel(
     const double2* __restrict__ rho, long long batch_stride_in, double2* __restrict__ G_out,
     double2* __restrict__ Hee_out, long long batch_stride_out, const double2* __restrict__ rho0p,
     const double* __restrict__ Wp, double2* __restrict__ diag0, const StageField* __restrict__ field,
@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(512) plane_rhs_kernel(
     const double2* src = rho + (long long)b * batch_stride_in + (long long)p * Nk;
     for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
     __syncthreads();
-    plane_forward<1>(X, 0, pl, roots);
+    plane_forward<1, MASK>(X, 0, pl, roots);
 
     const StageField F = field[b];
     const int n = p / nb, m = p - (p / nb) * nb;
@@ -73,8 +73,9 @@ __global__ void __launch_bounds__(512) plane_rhs_kernel(
         }
     }
     __syncthreads();
-    if (COUL) plane_inverse<2>(X, Nk, pl, roots);
-    else plane_inverse<1>(X, 0, pl, roots);
+    // the two inverse transforms run one after the other (fewer live registers)
+    plane_inverse<1, MASK>(X, 0, pl, roots);
+    if (COUL) plane_inverse<1, MASK>(Y, 0, pl, roots);
 
     double2* gdst = G_out + (long long)b * batch_stride_out + (long long)p * Nk;
     for (int i = threadIdx.x; i < Nk; i += blockDim.x) gdst[i] = X[i];
@@ -82,6 +83,112 @@ __global__ void __launch_bounds__(512) plane_rhs_kernel(
         double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
         for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = Y[i];
     }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent single-buffer plane kernel: the same contract as plane_rhs_kernel
+// with one plane (16 Nk bytes) of shared memory, so two CTAs share an SM and
+// one CTA's transforms overlap the other's loads and stores.  CTA c works on
+// planes w = c, c + gridDim.x, ... of the P x B planes.  With HSEX the two
+// inverse transforms run in turn from one buffer; rho(R) survives the first
+// in the CTA's own slot of `scratch` ([gridDim.x][Nk], written and read back
+// by the same thread, so it stays in L2 and needs no fence).
+template <bool COUL, int MASK, int MAXT>
+__global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
+    const double2* __restrict__ rho, long long batch_stride_in, double2* __restrict__ G_out,
+    double2* __restrict__ Hee_out, long long batch_stride_out, const double2* __restrict__ rho0p,
+    const double* __restrict__ Wp, double2* __restrict__ diag0, const StageField* __restrict__ field,
+    const double2* __restrict__ roots, const double* __restrict__ rpos, PlanePlan pl, int nb, double inv_nk,
+    double2* __restrict__ scratch, int nplanes) {
+    extern __shared__ double2 smem[];
+    const int Nk = pl.Nk;
+    const int P = nb * nb;
+    double2* X = smem;
+    double2* slot = scratch + (long long)blockIdx.x * Nk;
+    const int n1 = pl.ax[1].n, n2 = pl.ax[2].n;
+    const double* rp0 = rpos + pl.ax[0].rposoff;
+    const double* rp1 = rpos + pl.ax[1].rposoff;
+    const double* rp2 = rpos + pl.ax[2].rposoff;
+    for (int w = blockIdx.x; w < nplanes; w += gridDim.x) {
+        const int b = w / P, p = w - (w / P) * P;
+        const double2* src = rho + (long long)b * batch_stride_in + (long long)p * Nk;
+        for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
+        __syncthreads();
+        plane_forward<1, MASK>(X, 0, pl, roots);
+        const StageField F = field[b];
+        const int n = p / nb, m = p - (p / nb) * nb;
+        if (COUL && n == m && threadIdx.x == 0) diag0[b * nb + n] = cscale(X[0], inv_nk);
+        __syncthreads();
+        for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
+            const int t = fdiv(j, pl.fd_n2);
+            const int q2 = j - t * n2;
+            const int q0 = fdiv(t, pl.fd_n1);
+            const int q1 = t - q0 * n1;
+            const double dot = F.g[0] * __ldg(&rp0[q0]) + F.g[1] * __ldg(&rp1[q1]) + F.g[2] * __ldg(&rp2[q2]);
+            const double2 r = cscale(X[j], inv_nk);
+            if (COUL) slot[j] = r;
+            X[j] = make_double2(-dot * r.y, dot * r.x);
+        }
+        __syncthreads();
+        plane_inverse<1, MASK>(X, 0, pl, roots);
+        double2* gdst = G_out + (long long)b * batch_stride_out + (long long)p * Nk;
+        for (int i = threadIdx.x; i < Nk; i += blockDim.x) gdst[i] = X[i];
+        if (COUL) {
+            __syncthreads();  // the stores above read X before it is refilled
+            const double2* r0p = rho0p + (long long)p * Nk;
+            const double* wp = Wp + (long long)p * Nk;
+            for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
+                const double2 r = slot[j];
+                const double2 r0 = __ldg(&r0p[j]);
+                const double wv = __ldg(&wp[j]);
+                X[j] = make_double2(-wv * (r.x - r0.x), -wv * (r.y - r0.y));
+            }
+            __syncthreads();
+            plane_inverse<1, MASK>(X, 0, pl, roots);
+            double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
+            for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = X[i];
+        }
+        __syncthreads();  // X is reloaded by the next plane
+    }
+}
+
+// Plane-kernel variants: the generic one (every radix, up to 512 threads) and
+// one specialised for plans made of radices 8 and 9 (72-point axes), which
+// fits up to 768 threads.  The thread count is chosen per plan so that the
+// butterflies of each stage split into as few, as full, rounds as possible.
+struct PlaneLaunch {
+    int variant;  // 0 generic, 1 radix {8,9}
+    int threads;
+    bool persist;  // persistent single-buffer kernel, two CTAs per SM
+};
+
+inline PlaneLaunch plane_launch(const PlanePlan& pl) {
+    bool only89 = true;
+    for (int d = 0; d < 3; ++d)
+        for (int s = 0; s < pl.ax[d].nst; ++s)
+            if (pl.ax[d].r[s] != 8 && pl.ax[d].r[s] != 9) only89 = false;
+    PlaneLaunch L;
+    L.variant = only89 ? 1 : 0;
+    // two single-plane CTAs per SM when a plane leaves room for a second one
+    L.persist = (size_t)pl.Nk * 16 <= 110 * 1024;
+    const int tmax = L.persist ? (only89 ? 384 : 256) : (only89 ? 768 : 512);
+    long best = -1;
+    L.threads = tmax;
+    for (int T = 128; T <= tmax; T += 32) {
+        long cost = 0;
+        for (int d = 0; d < 3; ++d)
+            for (int s = 0; s < pl.ax[d].nst; ++s) {
+                const int r = pl.ax[d].r[s];
+                const long tasks = pl.Nk / r;
+                cost += ((tasks + T - 1) / T) * (long)r;
+            }
+        cost = cost * 4 + 3 * ((pl.Nk + T - 1) / T);  // stages (3 transforms) + load/pointwise/store
+        if (best < 0 || cost <= best) {
+            best = cost;
+            L.threads = T;
+        }
+    }
+    return L;
 }
 
 // ---------------------------------------------------------------------------
@@ -147,10 +254,118 @@ __host__ __device__ inline CommGeom comm_geometry(int nb) {
     return g;
 }
 
+// Stage inputs of a (k tile, solve) into shared memory: H = H0 + sum_d E_d xi_d
+// (+ Hee + Hartree diagonal) and rho, element (p, kk) handed to store(i, j, kk, h, r).
+// Elements are taken U at a time with every global load issued before any is
+// used, so that each thread keeps several loads in flight.
+template <bool COUL, typename Store>
+__device__ __forceinline__ void load_stage_inputs(const StageArgs& a, const StageField& F, const double2* hh, int b,
+                                                  int k0, Store store) {
+    constexpr int U = 4;
+    const int nb = a.nb, P = nb * nb, TK = a.TK, Nk = a.Nk;
+    const long long boff = (long long)b * a.bstride;
+    const int total = P * TK;
+    const bool e0 = F.E[0] != 0.0, e1 = F.E[1] != 0.0, e2 = F.E[2] != 0.0;
+    for (int base = threadIdx.x; base < total; base += U * blockDim.x) {
+        double2 r[U], h[U], x0[U], x1[U], x2[U], he[U];
+        long long el[U];
+        bool ok[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int idx = base + u * blockDim.x;
+            const int p = idx / TK, kk = idx - (idx / TK) * TK;
+            ok[u] = idx < total && k0 + kk < Nk;
+            el[u] = (long long)p * Nk + k0 + kk;
+            if (ok[u]) {
+                r[u] = __ldg(&a.rho[boff + el[u]]);
+                h[u] = __ldg(&a.H0[el[u]]);
+                if (e0) x0[u] = __ldg(&a.xi[0][el[u]]);
+                if (e1) x1[u] = __ldg(&a.xi[1][el[u]]);
+                if (e2) x2[u] = __ldg(&a.xi[2][el[u]]);
+                if (COUL) he[u] = __ldg(&a.Hee[boff + el[u]]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int idx = base + u * blockDim.x;
+            if (idx >= total) continue;
+            const int p = idx / TK, kk = idx - (idx / TK) * TK;
+            const int i = p / nb, j = p - (p / nb) * nb;
+            double2 hv = make_double2(0.0, 0.0), rv = make_double2(0.0, 0.0);
+            if (ok[u]) {
+                hv = h[u];
+                rv = r[u];
+                if (e0) { hv.x += F.E[0] * x0[u].x; hv.y += F.E[0] * x0[u].y; }
+                if (e1) { hv.x += F.E[1] * x1[u].x; hv.y += F.E[1] * x1[u].y; }
+                if (e2) { hv.x += F.E[2] * x2[u].x; hv.y += F.E[2] * x2[u].y; }
+                if (COUL) {
+                    hv = cadd(hv, he[u]);
+                    if (i == j) hv = cadd(hv, hh[i]);
+                }
+            }
+            store(i, j, kk, hv, rv);
+        }
+    }
+}
+
+// f = G - i C from the staged commutator Cs [P][TK], then the stage update,
+// U elements at a time with all loads issued first.
+template <int MODE>
+__device__ __forceinline__ void stage_epilogue(const StageArgs& a, const double2* Cs, int b, int k0) {
+    constexpr int U = 4;
+    const int nb = a.nb, P = nb * nb, TK = a.TK, Nk = a.Nk;
+    const long long boff = (long long)b * a.bstride;
+    const int total = P * TK;
+    for (int base = threadIdx.x; base < total; base += U * blockDim.x) {
+        double2 g[U], y[U], ac[U];
+        long long el[U];
+        bool ok[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int idx = base + u * blockDim.x;
+            const int p = idx / TK, kk = idx - (idx / TK) * TK;
+            ok[u] = idx < total && k0 + kk < Nk;
+            el[u] = boff + (long long)p * Nk + k0 + kk;
+            if (ok[u]) {
+                g[u] = __ldg(&a.G[el[u]]);
+                if (MODE == MODE_RK1 || MODE == MODE_RK2 || MODE == MODE_RK3 || MODE == MODE_AB) y[u] = a.y[el[u]];
+                if (MODE == MODE_RK2 || MODE == MODE_RK3 || MODE == MODE_RK4) ac[u] = a.acc[el[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (!ok[u]) continue;
+            const double2 c = Cs[base + u * blockDim.x];
+            const long long e = el[u];
+            // f = G - i C
+            const double2 f = make_double2(g[u].x + c.y, g[u].y - c.x);
+            if (MODE == MODE_RHS) {
+                a.out[e] = f;
+            } else if (MODE == MODE_RK1) {
+                a.aux[e] = make_double2(y[u].x + a.c[0] * f.x, y[u].y + a.c[0] * f.y);
+                a.acc[e] = make_double2(y[u].x + a.c[1] * f.x, y[u].y + a.c[1] * f.y);
+            } else if (MODE == MODE_RK2 || MODE == MODE_RK3) {
+                a.aux[e] = make_double2(y[u].x + a.c[0] * f.x, y[u].y + a.c[0] * f.y);
+                a.acc[e] = make_double2(ac[u].x + a.c[1] * f.x, ac[u].y + a.c[1] * f.y);
+            } else if (MODE == MODE_RK4) {
+                a.y[e] = make_double2(ac[u].x + a.c[0] * f.x, ac[u].y + a.c[0] * f.y);
+            } else if (MODE == MODE_AB) {
+                a.hist[0][e] = f;
+                double2 yy = make_double2(y[u].x + a.c[0] * f.x, y[u].y + a.c[0] * f.y);
+                for (int q = 1; q < a.order; ++q) {
+                    const double2 fq = a.hist[q][e];
+                    yy = make_double2(yy.x + a.c[q] * fq.x, yy.y + a.c[q] * fq.y);
+                }
+                a.y[e] = yy;
+            }
+        }
+    }
+}
+
 template <int MODE, bool COUL>
 __global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
     extern __shared__ double2 sm[];
-    const int nb = a.nb, P = nb * nb, TK = a.TK, Nk = a.Nk;
+    const int nb = a.nb, TK = a.TK;
     const int nbp = (nb + 1) & ~1, ld = nbp + 1;
     const int tile_stride = nbp * ld;
     double2* Hs = sm;                        // [TK][nbp][ld]
@@ -159,7 +374,6 @@ __global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
     double2* Cs = sm;                        // [P][TK], over Hs once the products are done
     const int b = blockIdx.y;
     const int k0 = blockIdx.x * TK;
-    const long long boff = (long long)b * a.bstride;
     const StageField F = a.field[b];
     if (COUL) {
         for (int n = threadIdx.x; n < nb; n += blockDim.x) {
@@ -173,28 +387,11 @@ __global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
         }
         __syncthreads();
     }
-    const bool e0 = F.E[0] != 0.0, e1 = F.E[1] != 0.0, e2 = F.E[2] != 0.0;
-    for (int idx = threadIdx.x; idx < P * TK; idx += blockDim.x) {
-        const int p = idx / TK, kk = idx - (idx / TK) * TK;
-        const int k = k0 + kk;
-        double2 h = make_double2(0.0, 0.0), r = make_double2(0.0, 0.0);
-        const int i = p / nb, j = p - (p / nb) * nb;
-        if (k < Nk) {
-            const long long e = (long long)p * Nk + k;
-            r = __ldg(&a.rho[boff + e]);
-            h = __ldg(&a.H0[e]);
-            if (e0) { double2 x = __ldg(&a.xi[0][e]); h.x += F.E[0] * x.x; h.y += F.E[0] * x.y; }
-            if (e1) { double2 x = __ldg(&a.xi[1][e]); h.x += F.E[1] * x.x; h.y += F.E[1] * x.y; }
-            if (e2) { double2 x = __ldg(&a.xi[2][e]); h.x += F.E[2] * x.x; h.y += F.E[2] * x.y; }
-            if (COUL) {
-                h = cadd(h, __ldg(&a.Hee[boff + e]));
-                if (i == j) h = cadd(h, hh[i]);
-            }
-        }
+    load_stage_inputs<COUL>(a, F, hh, b, k0, [&](int i, int j, int kk, double2 h, double2 r) {
         const int o = kk * tile_stride + i * ld + j;
         Hs[o] = h;
         Rs[o] = r;
-    }
+    });
     __syncthreads();
     // C = H rho - rho H on 2x2 tiles (rows i0, i0+1; columns j0, j0+1) of one
     // k point: per l, 8 shared loads feed 8 complex multiply-adds.
@@ -258,40 +455,7 @@ __global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
         }
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < P * TK; idx += blockDim.x) {
-        const int p = idx / TK, kk = idx - (idx / TK) * TK;
-        const int k = k0 + kk;
-        if (k >= Nk) continue;
-        const double2 c = Cs[idx];
-        const long long e = boff + (long long)p * Nk + k;
-        const double2 g = __ldg(&a.G[e]);
-        // f = G - i C
-        const double2 f = make_double2(g.x + c.y, g.y - c.x);
-        if (MODE == MODE_RHS) {
-            a.out[e] = f;
-        } else if (MODE == MODE_RK1) {
-            const double2 y = a.y[e];
-            a.aux[e] = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
-            a.acc[e] = make_double2(y.x + a.c[1] * f.x, y.y + a.c[1] * f.y);
-        } else if (MODE == MODE_RK2 || MODE == MODE_RK3) {
-            const double2 y = a.y[e];
-            const double2 ac = a.acc[e];
-            a.aux[e] = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
-            a.acc[e] = make_double2(ac.x + a.c[1] * f.x, ac.y + a.c[1] * f.y);
-        } else if (MODE == MODE_RK4) {
-            const double2 ac = a.acc[e];
-            a.y[e] = make_double2(ac.x + a.c[0] * f.x, ac.y + a.c[0] * f.y);
-        } else if (MODE == MODE_AB) {
-            a.hist[0][e] = f;
-            double2 y = a.y[e];
-            y = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
-            for (int q = 1; q < a.order; ++q) {
-                const double2 fq = a.hist[q][e];
-                y = make_double2(y.x + a.c[q] * fq.x, y.y + a.c[q] * fq.y);
-            }
-            a.y[e] = y;
-        }
-    }
+    stage_epilogue<MODE>(a, Cs, b, k0);
 }
 
 // ---------------------------------------------------------------------------
@@ -355,9 +519,9 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 }
 
 template <int MODE, bool COUL>
-__global__ void __launch_bounds__(256) commutator_mma_kernel(StageArgs a) {
+__global__ void __launch_bounds__(256, 2) commutator_mma_kernel(StageArgs a) {
     extern __shared__ double smd[];
-    const int nb = a.nb, P = nb * nb, Nk = a.Nk;
+    const int nb = a.nb, Nk = a.Nk;
     const MmaGeom g = mma_geometry(nb);
     const int TK = g.TK, nbp = g.nbp, pitch = g.pitch;
     const int mat = nbp * pitch;  // doubles per matrix
@@ -366,7 +530,6 @@ __global__ void __launch_bounds__(256) commutator_mma_kernel(StageArgs a) {
     double2* Cs = (double2*)smd;  // [P][TK] after the products
     const int b = blockIdx.y;
     const int k0 = blockIdx.x * TK;
-    const long long boff = (long long)b * a.bstride;
     const StageField F = a.field[b];
     for (int i = threadIdx.x; i < TK * 4 * mat; i += blockDim.x) tiles[i] = 0.0;
     if (COUL) {
@@ -381,28 +544,13 @@ __global__ void __launch_bounds__(256) commutator_mma_kernel(StageArgs a) {
         }
     }
     __syncthreads();
-    const bool e0 = F.E[0] != 0.0, e1 = F.E[1] != 0.0, e2 = F.E[2] != 0.0;
-    for (int idx = threadIdx.x; idx < P * TK; idx += blockDim.x) {
-        const int p = idx / TK, kk = idx - (idx / TK) * TK;
-        const int k = k0 + kk;
-        if (k >= Nk) continue;
-        const int i = p / nb, j = p - (p / nb) * nb;
-        const long long e = (long long)p * Nk + k;
-        const double2 r = __ldg(&a.rho[boff + e]);
-        double2 h = __ldg(&a.H0[e]);
-        if (e0) { double2 x = __ldg(&a.xi[0][e]); h.x += F.E[0] * x.x; h.y += F.E[0] * x.y; }
-        if (e1) { double2 x = __ldg(&a.xi[1][e]); h.x += F.E[1] * x.x; h.y += F.E[1] * x.y; }
-        if (e2) { double2 x = __ldg(&a.xi[2][e]); h.x += F.E[2] * x.x; h.y += F.E[2] * x.y; }
-        if (COUL) {
-            h = cadd(h, __ldg(&a.Hee[boff + e]));
-            if (i == j) h = cadd(h, hh[i]);
-        }
+    load_stage_inputs<COUL>(a, F, hh, b, k0, [&](int i, int j, int kk, double2 h, double2 r) {
         double* T = tiles + (size_t)kk * 4 * mat + i * pitch + j;
         T[0] = h.x;
         T[mat] = h.y;
         T[2 * mat] = r.x;
         T[3 * mat] = r.y;
-    }
+    });
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kk = warp / g.warps_per_k, part = warp - kk * g.warps_per_k;
@@ -463,39 +611,7 @@ __global__ void __launch_bounds__(256) commutator_mma_kernel(StageArgs a) {
         }
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < P * TK; idx += blockDim.x) {
-        const int p = idx / TK, kq = idx - (idx / TK) * TK;
-        const int k = k0 + kq;
-        if (k >= Nk) continue;
-        const double2 c = Cs[idx];
-        const long long e = boff + (long long)p * Nk + k;
-        const double2 gg = __ldg(&a.G[e]);
-        const double2 f = make_double2(gg.x + c.y, gg.y - c.x);
-        if (MODE == MODE_RHS) {
-            a.out[e] = f;
-        } else if (MODE == MODE_RK1) {
-            const double2 y = a.y[e];
-            a.aux[e] = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
-            a.acc[e] = make_double2(y.x + a.c[1] * f.x, y.y + a.c[1] * f.y);
-        } else if (MODE == MODE_RK2 || MODE == MODE_RK3) {
-            const double2 y = a.y[e];
-            const double2 ac2 = a.acc[e];
-            a.aux[e] = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
-            a.acc[e] = make_double2(ac2.x + a.c[1] * f.x, ac2.y + a.c[1] * f.y);
-        } else if (MODE == MODE_RK4) {
-            const double2 ac2 = a.acc[e];
-            a.y[e] = make_double2(ac2.x + a.c[0] * f.x, ac2.y + a.c[0] * f.y);
-        } else if (MODE == MODE_AB) {
-            a.hist[0][e] = f;
-            double2 y = a.y[e];
-            y = make_double2(y.x + a.c[0] * f.x, y.y + a.c[0] * f.y);
-            for (int q = 1; q < a.order; ++q) {
-                const double2 fq = a.hist[q][e];
-                y = make_double2(y.x + a.c[q] * fq.x, y.y + a.c[q] * fq.y);
-            }
-            a.y[e] = y;
-        }
-    }
+    stage_epilogue<MODE>(a, Cs, b, k0);
 }
 
 // ---------------------------------------------------------------------------
