@@ -14,6 +14,7 @@
 #include <stdexcept>
 #include "../../include/edus_gpu.h"
 #include "kernels.cuh"
+#include "packed_kernels.cuh"
 #include "plane_plan.hpp"
 
 using namespace edus;
@@ -77,6 +78,23 @@ struct edus_handle {
     std::vector<cudaEvent_t> prof_pool;
     double prof_ms[2] = {0, 0};
     unsigned long long prof_n[2] = {0, 0};
+    // packed-Hermitian forms (HERM64, MIXED)
+    bool packed = false, mixed = false;
+    int Pq = 0;
+    size_t Sq = 0;                      // Pq*Nk
+    int* qnm = nullptr;                 // packed plane -> (n << 16) | m
+    bool ref_fixed = false;
+    double2* ref_full = nullptr;        // rho_ref, FP64 full planes
+    void *pH0p = nullptr, *pxi[3] = {nullptr, nullptr, nullptr}, *pRref = nullptr;  // ST planes
+    void* pW = nullptr;                 // packed, digit-reversed W (real, ST scalar)
+    double2 *pC0 = nullptr, *pK[3] = {nullptr, nullptr, nullptr};
+    double2 *py = nullptr, *pacc = nullptr, *phist[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    void *paux = nullptr, *pG = nullptr, *pE1 = nullptr;
+    double2* pdiag0 = nullptr;          // [B][nb] delta_nn(R=0)
+    StageField* ref_fields = nullptr;   // E = 0, e_x, e_y, e_z
+    PackedGeom pgeo{};
+    int pplane_threads = 256, pplane_variant = 0;
+    size_t pplane_smem = 0;
 };
 
 namespace {
@@ -280,6 +298,217 @@ StageArgs base_args(edus_handle* h) {
     return a;
 }
 
+
+// ---------------------------------------------------------------------------
+// packed-Hermitian forms: launch helpers
+
+template <typename C, typename IT, bool COUL>
+void pplane_t(edus_handle* h, const IT* in, const StageField* field, int nbatch) {
+    dim3 grid(h->Pq, nbatch);
+    using T = typename CplxT<C>::T;
+    const long long bs = (long long)h->Sq;
+    if (h->pplane_variant == 1)
+        plane_packed_kernel<C, IT, kRadix89, 512, COUL><<<grid, h->pplane_threads, h->pplane_smem, h->stream>>>(
+            in, bs, (C*)h->pG, (C*)h->pE1, bs, (const T*)h->pW, h->pdiag0, field, h->roots, h->rpos, h->plan, h->qnm,
+            h->nb, 1.0 / h->Nk);
+    else
+        plane_packed_kernel<C, IT, kRadixAll, 512, COUL><<<grid, h->pplane_threads, h->pplane_smem, h->stream>>>(
+            in, bs, (C*)h->pG, (C*)h->pE1, bs, (const T*)h->pW, h->pdiag0, field, h->roots, h->rpos, h->plan, h->qnm,
+            h->nb, 1.0 / h->Nk);
+}
+
+// in_is_aux: the input is the RK stage input (FP32 in MIXED), else the FP64 state
+int launch_pplane(edus_handle* h, const void* in, bool in_is_aux, const StageField* field, int nbatch) {
+    cudaEvent_t e0;
+    prof_begin(h, &e0);
+    const bool c = h->d.coulomb != 0;
+    if (h->mixed) {
+        if (in_is_aux) {
+            if (c) pplane_t<float2, float2, true>(h, (const float2*)in, field, nbatch);
+            else pplane_t<float2, float2, false>(h, (const float2*)in, field, nbatch);
+        } else {
+            if (c) pplane_t<float2, double2, true>(h, (const double2*)in, field, nbatch);
+            else pplane_t<float2, double2, false>(h, (const double2*)in, field, nbatch);
+        }
+    } else {
+        if (c) pplane_t<double2, double2, true>(h, (const double2*)in, field, nbatch);
+        else pplane_t<double2, double2, false>(h, (const double2*)in, field, nbatch);
+    }
+    h->launches++;
+    CU(h, cudaGetLastError());
+    prof_end(h, 0, e0);
+    return EDUS_OK;
+}
+
+template <int MODE, bool COUL, typename ST, typename IT, typename AT>
+void pcomm_t(edus_handle* h, const PackedArgs& a, int nbatch) {
+    dim3 grid((h->Nk + h->pgeo.TK - 1) / h->pgeo.TK, nbatch);
+    commutator_packed_kernel<MODE, COUL, ST, IT, AT><<<grid, 256, h->pgeo.smem, h->stream>>>(a);
+}
+
+template <int MODE, bool COUL>
+void pcomm_mode(edus_handle* h, const PackedArgs& a, int nbatch) {
+    if (h->mixed) {
+        // RK stage 1 and AB read the FP64 state; RK stages 2-4 read the FP32 stage input
+        if (MODE == MODE_RK1 || MODE == MODE_AB || MODE == MODE_RHS)
+            pcomm_t<MODE, COUL, float2, double2, float2>(h, a, nbatch);
+        else
+            pcomm_t<MODE, COUL, float2, float2, float2>(h, a, nbatch);
+    } else {
+        pcomm_t<MODE, COUL, double2, double2, double2>(h, a, nbatch);
+    }
+}
+
+int launch_pcomm(edus_handle* h, int mode, const PackedArgs& a, int nbatch) {
+    cudaEvent_t e0;
+    prof_begin(h, &e0);
+    const bool c = h->d.coulomb != 0;
+#define PC(M)                                          \
+    case M:                                            \
+        if (c) pcomm_mode<M, true>(h, a, nbatch);      \
+        else pcomm_mode<M, false>(h, a, nbatch);       \
+        break;
+    switch (mode) {
+        PC(MODE_RK1) PC(MODE_RK2) PC(MODE_RK3) PC(MODE_RK4) PC(MODE_AB)
+        default: return fail(h, EDUS_ERR_ARG, "bad packed stage mode");
+    }
+#undef PC
+    h->launches++;
+    CU(h, cudaGetLastError());
+    prof_end(h, 1, e0);
+    return EDUS_OK;
+}
+
+template <typename K>
+int set_smem_any(edus_handle* h, K kernel, size_t bytes) {
+    CU(h, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return EDUS_OK;
+}
+
+template <int MODE, bool COUL>
+int set_pcomm_smem(edus_handle* h) {
+    int rc;
+    if ((rc = set_smem_any(h, commutator_packed_kernel<MODE, COUL, float2, double2, float2>, h->pgeo.smem))) return rc;
+    if ((rc = set_smem_any(h, commutator_packed_kernel<MODE, COUL, float2, float2, float2>, h->pgeo.smem))) return rc;
+    if ((rc = set_smem_any(h, commutator_packed_kernel<MODE, COUL, double2, double2, double2>, h->pgeo.smem))) return rc;
+    return EDUS_OK;
+}
+
+template <typename C, typename IT, bool COUL>
+int set_pplane_smem(edus_handle* h) {
+    int rc;
+    if ((rc = set_smem_any(h, plane_packed_kernel<C, IT, kRadix89, 512, COUL>, h->pplane_smem))) return rc;
+    if ((rc = set_smem_any(h, plane_packed_kernel<C, IT, kRadixAll, 512, COUL>, h->pplane_smem))) return rc;
+    return EDUS_OK;
+}
+
+int packed_setup_smem(edus_handle* h) {
+    int rc;
+#define SP(M)                                                   \
+    if ((rc = set_pcomm_smem<M, true>(h))) return rc;           \
+    if ((rc = set_pcomm_smem<M, false>(h))) return rc;
+    SP(MODE_RK1) SP(MODE_RK2) SP(MODE_RK3) SP(MODE_RK4) SP(MODE_AB)
+#undef SP
+    if ((rc = set_pplane_smem<float2, double2, true>(h))) return rc;
+    if ((rc = set_pplane_smem<float2, double2, false>(h))) return rc;
+    if ((rc = set_pplane_smem<float2, float2, true>(h))) return rc;
+    if ((rc = set_pplane_smem<float2, float2, false>(h))) return rc;
+    if ((rc = set_pplane_smem<double2, double2, true>(h))) return rc;
+    if ((rc = set_pplane_smem<double2, double2, false>(h))) return rc;
+    return EDUS_OK;
+}
+
+int grid_for(long long n) { return (int)std::min<long long>((n + 255) / 256, 148LL * 8); }
+
+// rho_ref := the full-plane state y[b]; C0, K_d, H0' from the FP64 full-plane
+// kernels, then packed (and rounded to the storage type).
+int fix_reference(edus_handle* h, int b) {
+    int rc;
+    const size_t Sb = h->S * sizeof(double2);
+    if (!h->tmp_in) {
+        if ((rc = dalloc(h, (void**)&h->tmp_in, Sb))) return rc;
+        if ((rc = dalloc(h, (void**)&h->tmp_out, Sb))) return rc;
+    }
+    CU(h, cudaMemcpyAsync(h->ref_full, h->y + (size_t)b * h->S, Sb, cudaMemcpyDeviceToDevice, h->stream));
+    StageField rf[4];
+    for (int f = 0; f < 4; ++f) {
+        for (int d = 0; d < 3; ++d) rf[f].E[d] = (f == d + 1) ? 1.0 : 0.0;
+        for (int c = 0; c < 3; ++c) rf[f].g[c] = h->A[0 * 3 + c] * rf[f].E[0] + h->A[1 * 3 + c] * rf[f].E[1] + h->A[2 * 3 + c] * rf[f].E[2];
+    }
+    CU(h, cudaMemcpyAsync(h->ref_fields, rf, sizeof(rf), cudaMemcpyHostToDevice, h->stream));
+    // E = 0: Hee(rho_ref), rho_ref diagonal at R = 0, then C0 = f(rho_ref; 0)
+    if ((rc = launch_plane(h, h->ref_full, 0, h->G, h->Hee, 0, h->ref_fields, 1))) return rc;
+    const int coul = h->d.coulomb ? 1 : 0;
+    const long long nS = (long long)h->S;
+    assemble_h0p<<<grid_for(nS), 256, 0, h->stream>>>(h->H0, h->Hee, h->tmp_in, h->hartree, h->diag0, h->rho0diag,
+                                                       h->nb, h->Nk, coul);
+    h->launches++;
+    StageArgs a = base_args(h);
+    a.rho = h->ref_full;
+    a.field = h->ref_fields;
+    a.out = h->tmp_out;
+    if ((rc = launch_comm(h, MODE_RHS, a, 1))) return rc;  // tmp_out = C0 (full)
+    const long long nq = (long long)h->Sq;
+    pack_planes<double2><<<grid_for(nq), 256, 0, h->stream>>>(h->tmp_out, h->pC0, h->qnm, h->nb, h->Pq, h->Nk);
+    h->launches++;
+    for (int d = 0; d < 3; ++d) {
+        if ((rc = launch_plane(h, h->ref_full, 0, h->G, h->Hee, 0, h->ref_fields + 1 + d, 1))) return rc;
+        a.field = h->ref_fields + 1 + d;
+        a.out = h->stage;
+        if ((rc = launch_comm(h, MODE_RHS, a, 1))) return rc;  // stage = f(rho_ref; e_d)
+        sub_planes<<<grid_for(nS), 256, 0, h->stream>>>(h->stage, h->tmp_out, h->stage, nS);
+        pack_planes<double2><<<grid_for(nq), 256, 0, h->stream>>>(h->stage, h->pK[d], h->qnm, h->nb, h->Pq, h->Nk);
+        h->launches += 2;
+    }
+    if (h->mixed) {
+        pack_planes<float2><<<grid_for(nq), 256, 0, h->stream>>>(h->tmp_in, (float2*)h->pH0p, h->qnm, h->nb, h->Pq, h->Nk);
+        pack_planes<float2><<<grid_for(nq), 256, 0, h->stream>>>(h->ref_full, (float2*)h->pRref, h->qnm, h->nb, h->Pq, h->Nk);
+    } else {
+        pack_planes<double2><<<grid_for(nq), 256, 0, h->stream>>>(h->tmp_in, (double2*)h->pH0p, h->qnm, h->nb, h->Pq, h->Nk);
+        pack_planes<double2><<<grid_for(nq), 256, 0, h->stream>>>(h->ref_full, (double2*)h->pRref, h->qnm, h->nb, h->Pq, h->Nk);
+    }
+    h->launches += 2;
+    CU(h, cudaGetLastError());
+    CU(h, cudaStreamSynchronize(h->stream));
+    h->ref_fixed = true;
+    return EDUS_OK;
+}
+
+PackedArgs base_pargs(edus_handle* h) {
+    PackedArgs a{};
+    a.G = h->pG;
+    a.E1 = h->pE1;
+    a.H0p = h->pH0p;
+    for (int d = 0; d < 3; ++d) {
+        a.xi[d] = h->pxi[d];
+        a.K[d] = h->pK[d];
+    }
+    a.Rref = h->pRref;
+    a.C0 = h->pC0;
+    a.hartree = h->hartree;
+    a.diag0 = h->pdiag0;
+    a.qnm = h->qnm;
+    a.y = h->py;
+    a.aux = h->paux;
+    a.acc = h->pacc;
+    a.bstride = (long long)h->Sq;
+    a.Nk = h->Nk;
+    a.nb = h->nb;
+    a.Pq = h->Pq;
+    a.TK = h->pgeo.TK;
+    return a;
+}
+
+// the state y[b] (full FP64 planes) from rho_ref + delta_b
+int unpack_state(edus_handle* h, int b) {
+    const long long nS = (long long)h->S;
+    unpack_delta<<<grid_for(nS), 256, 0, h->stream>>>(h->py + (size_t)b * h->Sq, h->ref_full, h->y + (size_t)b * h->S,
+                                                       h->nb, h->Nk);
+    h->launches++;
+    CU(h, cudaGetLastError());
+    return EDUS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -301,7 +530,10 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
         return fail(nullptr, EDUS_ERR_UNSUPPORTED, "RK is implemented for order 4 only (DESolver.hpp:157)");
     if (d.solver == EDUS_SOLVER_AB && d.order != 4 && d.order != 5)
         return fail(nullptr, EDUS_ERR_UNSUPPORTED, "order not implemented for AB (DESolver.hpp:120-124)");
-    if (d.precision != EDUS_PREC_FP64) return fail(nullptr, EDUS_ERR_UNSUPPORTED, "precision not supported");
+    if (d.precision != EDUS_PREC_FP64 && d.precision != EDUS_PREC_HERM64 && d.precision != EDUS_PREC_MIXED)
+        return fail(nullptr, EDUS_ERR_UNSUPPORTED, "precision not supported");
+    if (d.precision != EDUS_PREC_FP64 && d.nbands > 32)
+        return fail(nullptr, EDUS_ERR_UNSUPPORTED, "the packed-Hermitian forms handle up to 32 bands");
     if (d.batch < 1) return fail(nullptr, EDUS_ERR_ARG, "batch must be >= 1");
     if (!(d.dt > 0.0) || !std::isfinite(d.dt)) return fail(nullptr, EDUS_ERR_ARG, "dt must be positive and finite");
 
@@ -331,7 +563,18 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
         if (!build_plane_plan(h->N, h->plan, tabs, perr)) return bail(fail(h, EDUS_ERR_UNSUPPORTED, perr));
     }
     const std::vector<double2>& roots = tabs.roots;
-    const std::vector<double>& rpos = tabs.rpos;
+    std::vector<double>& rpos = tabs.rpos;
+    if (d.precision != EDUS_PREC_FP64) {
+        // The packed forms propagate the Hermitian part of the generator: on an
+        // even axis the Gamma-centred index N/2 is -N/2 for both R and -R, so
+        // the gradient's i (R.E) is not anti-Hermitian there; its Hermitian
+        // part has coordinate 0 on that index.
+        for (int ax = 0; ax < 3; ++ax)
+            for (int q = 0; q < h->N[ax]; ++q) {
+                double& x = rpos[h->plan.ax[ax].rposoff + q];
+                if (h->N[ax] % 2 == 0 && x == -0.5 * h->N[ax]) x = 0.0;
+            }
+    }
 
     int dev_smem = 0;
     cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, d.device);
@@ -414,6 +657,69 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     if (h->plane_cfg.persist && d.coulomb) TRY_ALLOC(h->plane_scratch, (size_t)h->plane_grid * h->Nk * sizeof(double2));
     TRY_ALLOC(h->popbuf, h->nb * sizeof(double));
     TRY_ALLOC(h->flag, sizeof(int));
+    if (d.precision != EDUS_PREC_FP64) {
+        h->packed = true;
+        h->mixed = d.precision == EDUS_PREC_MIXED;
+        h->Pq = h->nb * (h->nb + 1) / 2;
+        h->Sq = (size_t)h->Pq * h->Nk;
+        const size_t st = h->mixed ? sizeof(float2) : sizeof(double2);
+        const size_t sc = h->mixed ? sizeof(float) : sizeof(double);
+        const size_t Sq8 = h->Sq * sizeof(double2), SqB8 = Sq8 * h->B;
+        TRY_ALLOC(h->qnm, h->Pq * sizeof(int));
+        TRY_ALLOC(h->ref_full, Sb);
+        TRY_ALLOC(h->pH0p, h->Sq * st);
+        for (int i = 0; i < 3; ++i) TRY_ALLOC(h->pxi[i], h->Sq * st);
+        TRY_ALLOC(h->pRref, h->Sq * st);
+        TRY_ALLOC(h->pC0, Sq8);
+        for (int i = 0; i < 3; ++i) TRY_ALLOC(h->pK[i], Sq8);
+        TRY_ALLOC(h->py, SqB8);
+        TRY_ALLOC(h->pG, h->Sq * st * h->B);
+        if (d.coulomb) {
+            TRY_ALLOC(h->pE1, h->Sq * st * h->B);
+            TRY_ALLOC(h->pW, h->Sq * sc);
+            TRY_ALLOC(h->pdiag0, (size_t)h->B * h->nb * sizeof(double2));
+        }
+        if (d.solver == EDUS_SOLVER_RK) {
+            TRY_ALLOC(h->paux, h->Sq * st * h->B);
+            TRY_ALLOC(h->pacc, SqB8);
+        } else {
+            for (int i = 0; i < d.order; ++i) {
+                TRY_ALLOC(h->phist[i], SqB8);
+                if (cudaMemsetAsync(h->phist[i], 0, SqB8, h->stream) != cudaSuccess)
+                    return bail(fail(h, EDUS_ERR_CUDA, "cudaMemsetAsync failed"));
+            }
+        }
+        TRY_ALLOC(h->ref_fields, 4 * sizeof(StageField));
+        std::vector<int> qnm;
+        for (int n = 0; n < h->nb; ++n)
+            for (int m = n; m < h->nb; ++m) qnm.push_back((n << 16) | m);
+        if (cudaMemcpyAsync(h->qnm, qnm.data(), qnm.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+            return bail(fail(h, EDUS_ERR_CUDA, "upload of the packed plane map failed"));
+        h->pgeo = packed_geometry(h->nb);
+        const PlaneLaunch pl = plane_launch(h->plan);
+        h->pplane_variant = pl.variant;
+        // the packed transform: cost model over 128..512 threads
+        {
+            long best = -1;
+            for (int T = 128; T <= 512; T += 32) {
+                long cost = 0;
+                for (int ax = 0; ax < 3; ++ax)
+                    for (int s2 = 0; s2 < h->plan.ax[ax].nst; ++s2) {
+                        const int r = h->plan.ax[ax].r[s2];
+                        cost += ((h->Nk / r + T - 1) / T) * (long)r;
+                    }
+                cost = cost * 4 + 3 * ((h->Nk + T - 1) / T);
+                if (best < 0 || cost <= best) {
+                    best = cost;
+                    h->pplane_threads = T;
+                }
+            }
+        }
+        h->pplane_smem = (size_t)h->Nk * st * (d.coulomb ? 2 : 1);
+        if (h->pplane_smem > (size_t)dev_smem || h->pgeo.smem > (size_t)dev_smem)
+            return bail(fail(h, EDUS_ERR_UNSUPPORTED, "k grid too large for the packed plane kernel"));
+        if ((rc = packed_setup_smem(h))) return bail(rc);
+    }
 #undef TRY_ALLOC
     for (int i = 0; i < 2; ++i) {
         if (cudaMallocHost((void**)&h->field_host[i], (size_t)h->chunk * 4 * h->B * sizeof(StageField)) != cudaSuccess)
@@ -476,6 +782,40 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, co
             for (int s = 0; s < h->plan.ax[ax].nst; ++s) r.push_back(h->plan.ax[ax].r[s]);
             dif_positions(h->N[ax], r, fq[ax]);
         }
+        // W_R as uploaded; the packed forms take its Hermitian part
+        // (W_nm(R) + W_mn(-R)) / 2, which differs from W only on the planes
+        // where an even axis sits at its N/2 index (Gamma-centred to -N/2 for
+        // both R and -R).  Anywhere else an asymmetry is a model the packed
+        // forms cannot represent (e.g. two off-origin Wannier centres under
+        // the cumulative r of ModelCoulomb.cpp:76-79).
+        std::vector<double> Wuse;
+        if (h->packed) {
+            const int nb = h->nb;
+            Wuse.assign(h->S, 0.0);
+            double mx = 0, dev = 0;
+            for (int j0 = 0; j0 < h->N[0]; ++j0)
+                for (int j1 = 0; j1 < h->N[1]; ++j1)
+                    for (int j2 = 0; j2 < h->N[2]; ++j2) {
+                        const int j[3] = {j0, j1, j2};
+                        bool nyq = false;
+                        for (int ax = 0; ax < 3; ++ax) nyq |= (h->N[ax] % 2 == 0 && 2 * j[ax] == h->N[ax]);
+                        const int iR = (j0 * h->N[1] + j1) * h->N[2] + j2;
+                        const int mR = (((h->N[0] - j0) % h->N[0]) * h->N[1] + (h->N[1] - j1) % h->N[1]) * h->N[2] +
+                                       (h->N[2] - j2) % h->N[2];
+                        for (int n = 0; n < nb; ++n)
+                            for (int m = 0; m < nb; ++m) {
+                                const double a = W_R[2 * (((size_t)iR * nb + n) * nb + m)];
+                                const double c = W_R[2 * (((size_t)mR * nb + m) * nb + n)];
+                                mx = std::max(mx, std::fabs(a));
+                                if (!nyq) dev = std::max(dev, std::fabs(a - c));
+                                Wuse[((size_t)iR * nb + n) * nb + m] = 0.5 * (a + c);
+                            }
+                    }
+            if (dev > 1e-12 * std::max(mx, 1e-300))
+                return fail(h, EDUS_ERR_UNSUPPORTED,
+                            "the packed forms need W_nm(R) = W_mn(-R) (Hermitian self-energy); this model's Wannier "
+                            "centres break it (use EDUS_PREC_FP64)");
+        }
         std::vector<double> w(h->S);
         std::vector<double2> r0(h->S);
         const int N1 = h->N[1], N2 = h->N[2];
@@ -488,7 +828,7 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, co
                         const double* wsrc = W_R + 2 * ((size_t)iR * P + p);
                         if (wsrc[1] != 0.0)
                             return fail(h, EDUS_ERR_ARG, "W_R must be real (the screened potential has no imaginary part)");
-                        w[(size_t)p * Nk + pos] = wsrc[0];
+                        w[(size_t)p * Nk + pos] = h->packed ? Wuse[(size_t)iR * P + p] : wsrc[0];
                         const double* rsrc = rho0_R + 2 * ((size_t)iR * P + p);
                         r0[(size_t)p * Nk + pos] = make_double2(rsrc[0], rsrc[1]);
                     }
@@ -502,6 +842,42 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, co
         CU(h, cudaStreamSynchronize(h->stream));  // host vectors go out of scope
     }
     CU(h, cudaStreamSynchronize(h->stream));
+    if (h->packed) {
+        // the packed forms need Hermitian H0, xi and W_nm(R) = W_mn(-R)
+        const int nb = h->nb;
+        auto herm_ok = [&](const double* X) {
+            double mx = 0, dev = 0;
+            for (int k = 0; k < Nk; ++k)
+                for (int n = 0; n < nb; ++n)
+                    for (int m = n; m < nb; ++m) {
+                        const double* a = X + 2 * (((size_t)k * nb + n) * nb + m);
+                        const double* c = X + 2 * (((size_t)k * nb + m) * nb + n);
+                        mx = std::max(mx, std::fabs(a[0]) + std::fabs(a[1]));
+                        dev = std::max(dev, std::fabs(a[0] - c[0]) + std::fabs(a[1] + c[1]));
+                    }
+            return dev <= 1e-12 * std::max(mx, 1e-300);
+        };
+        if (!herm_ok(H0_k) || !herm_ok(xi_k) || !herm_ok(xi_k + 2 * h->S) || !herm_ok(xi_k + 4 * h->S))
+            return fail(h, EDUS_ERR_UNSUPPORTED, "the packed forms need Hermitian H0(k) and xi(k)");
+        const long long nq = (long long)h->Sq;
+        for (int dd = 0; dd < 3; ++dd) {
+            if (h->mixed)
+                pack_planes<float2><<<grid_for(nq), 256, 0, h->stream>>>(h->xi[dd], (float2*)h->pxi[dd], h->qnm, nb, h->Pq, Nk);
+            else
+                pack_planes<double2><<<grid_for(nq), 256, 0, h->stream>>>(h->xi[dd], (double2*)h->pxi[dd], h->qnm, nb, h->Pq, Nk);
+            h->launches++;
+        }
+        if (h->d.coulomb) {
+            if (h->mixed)
+                pack_scalar_planes<float><<<grid_for(nq), 256, 0, h->stream>>>(h->Wp, (float*)h->pW, h->qnm, nb, h->Pq, Nk);
+            else
+                pack_scalar_planes<double><<<grid_for(nq), 256, 0, h->stream>>>(h->Wp, (double*)h->pW, h->qnm, nb, h->Pq, Nk);
+            h->launches++;
+        }
+        CU(h, cudaGetLastError());
+        CU(h, cudaStreamSynchronize(h->stream));
+        h->ref_fixed = false;
+    }
     h->model_ready = true;
     return EDUS_OK;
 }
@@ -532,6 +908,16 @@ int edus_set_state(edus_handle* h, int b, const double* rho_k) {
     transpose_kp_to_pk<<<tg, tb, 0, h->stream>>>(h->stage, h->y + (size_t)b * h->S, h->Nk, h->P);
     h->launches++;
     CU(h, cudaGetLastError());
+    if (h->packed) {
+        if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "the packed forms need edus_upload_model before edus_set_state");
+        int rc;
+        if (!h->ref_fixed && (rc = fix_reference(h, b))) return rc;
+        const long long nq = (long long)h->Sq;
+        pack_delta<<<grid_for(nq), 256, 0, h->stream>>>(h->y + (size_t)b * h->S, h->ref_full, h->py + (size_t)b * h->Sq,
+                                                        h->qnm, h->nb, h->Pq, h->Nk);
+        h->launches++;
+        CU(h, cudaGetLastError());
+    }
     CU(h, cudaStreamSynchronize(h->stream));
     return EDUS_OK;
 }
@@ -540,6 +926,10 @@ int edus_get_state(edus_handle* h, int b, double* rho_k) {
     if (!h || !rho_k) return EDUS_ERR_ARG;
     if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
     CU(h, cudaSetDevice(h->d.device));
+    if (h->packed) {
+        int rc;
+        if ((rc = unpack_state(h, b))) return rc;
+    }
     dim3 tb(32, 8), tg((h->P + 31) / 32, (h->Nk + 31) / 32);
     transpose_pk_to_kp<<<tg, tb, 0, h->stream>>>(h->y + (size_t)b * h->S, h->stage, h->Nk, h->P);
     h->launches++;
@@ -624,6 +1014,42 @@ int edus_step(edus_handle* h, int n) {
         // kernels before this copy (same stream) have run
         CU(h, cudaMemcpyAsync(h->field, tab, (size_t)cnt * nst * B * sizeof(StageField), cudaMemcpyHostToDevice, h->stream));
         CU(h, cudaEventRecord(h->field_ev[buf], h->stream));
+        if (h->packed) {
+            if (!h->ref_fixed) return fail(h, EDUS_ERR_ARG, "the packed forms need edus_set_state before edus_step");
+            for (int i = 0; i < cnt; ++i) {
+                const StageField* fs = h->field + (size_t)i * nst * B;
+                PackedArgs a = base_pargs(h);
+                if (rk) {
+                    const double c0[4] = {dt / 2., dt / 2., dt, dt / 6.};
+                    const double c1[4] = {dt / 6., dt / 3., dt / 3., 0.};
+                    for (int s = 0; s < 4; ++s) {
+                        const void* in = (s == 0) ? (const void*)h->py : (const void*)h->paux;
+                        if ((rc = launch_pplane(h, in, s != 0, fs + (size_t)s * B, B))) return rc;
+                        a.in = in;
+                        a.field = fs + (size_t)s * B;
+                        a.c[0] = c0[s];
+                        a.c[1] = c1[s];
+                        if ((rc = launch_pcomm(h, MODE_RK1 + s, a, B))) return rc;
+                    }
+                } else {
+                    if ((rc = launch_pplane(h, h->py, false, fs, B))) return rc;
+                    a.in = h->py;
+                    a.field = fs;
+                    a.order = h->d.order;
+                    for (int q = 0; q < h->d.order; ++q) {
+                        a.hist[q] = h->phist[h->index[q]];
+                        a.c[q] = dt * h->beta[q];
+                    }
+                    if ((rc = launch_pcomm(h, MODE_AB, a, B))) return rc;
+                    const int ord = h->d.order;
+                    int tmp = h->index[ord - 1];
+                    for (int q = ord - 1; q > 0; --q) h->index[q] = h->index[q - 1];
+                    h->index[0] = tmp;
+                }
+                h->t += dt;
+            }
+            continue;
+        }
         for (int i = 0; i < cnt; ++i) {
             const StageField* fs = h->field + (size_t)i * nst * B;
             StageArgs a = base_args(h);
@@ -675,6 +1101,10 @@ int edus_population_wannier(edus_handle* h, int b, double* pop) {
     if (!h || !pop) return EDUS_ERR_ARG;
     if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
     CU(h, cudaSetDevice(h->d.device));
+    if (h->packed) {
+        int rc;
+        if ((rc = unpack_state(h, b))) return rc;
+    }
     population_kernel<<<h->nb, 256, 0, h->stream>>>(h->y + (size_t)b * h->S, h->Nk, h->nb, h->popbuf);
     h->launches++;
     CU(h, cudaGetLastError());

@@ -56,49 +56,80 @@ struct PlanePlan {
     FastDiv fd_n1, fd_n2;  // position -> (q0, q1, q2) in the pointwise stage
 };
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+// Complex helpers for double2 and float2 (the plane kernels run the FFT in
+// FP64 for the FP64 forms and in FP32 for the mixed-precision form).
+template <typename C>
+struct CplxT;
+template <>
+struct CplxT<double2> {
+    using T = double;
+};
+template <>
+struct CplxT<float2> {
+    using T = float;
+};
+
+__device__ __forceinline__ double2 mkc(double x, double y, double2*) { return make_double2(x, y); }
+__device__ __forceinline__ float2 mkc(float x, float y, float2*) { return make_float2(x, y); }
+template <typename C>
+__device__ __forceinline__ C cmake(typename CplxT<C>::T x, typename CplxT<C>::T y) {
+    return mkc(x, y, (C*)nullptr);
 }
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+    return cmake<C>(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) { return cmake<C>(a.x + b.x, a.y + b.y); }
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) { return cmake<C>(a.x - b.x, a.y - b.y); }
+template <typename C>
+__device__ __forceinline__ C cscale(C a, typename CplxT<C>::T s) { return cmake<C>(a.x * s, a.y * s); }
 // multiply by s*i (s = +1 or -1)
-template <int S>
-__device__ __forceinline__ double2 cmul_si(double2 a) {
-    return S > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+template <int S, typename C>
+__device__ __forceinline__ C cmul_si(C a) {
+    return S > 0 ? cmake<C>(-a.y, a.x) : cmake<C>(a.y, -a.x);
+}
+// root table entries are FP64; the FP32 transform rounds them once on use
+template <typename C>
+__device__ __forceinline__ C ldroot(const double2* p) {
+    const double2 w = __ldg(p);
+    return cmake<C>((typename CplxT<C>::T)w.x, (typename CplxT<C>::T)w.y);
 }
 
 // In-register DFT y_d = sum_b x_b exp(S 2 pi i b d / R), hand-coded radices.
-template <int R, int S>
+template <int R, int S, typename C>
 struct Dft;
 
-template <int S>
-struct Dft<2, S> {
-    __device__ __forceinline__ static void run(double2* v, const double2*, int) {
-        double2 a = v[0], b = v[1];
+template <int S, typename C>
+struct Dft<2, S, C> {
+    __device__ __forceinline__ static void run(C* v, const double2*, int) {
+        C a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
     }
 };
 
-template <int S>
-struct Dft<3, S> {
-    __device__ __forceinline__ static void run(double2* v, const double2*, int) {
-        const double h = 0.86602540378443864676;  // sqrt(3)/2
-        double2 t1 = cadd(v[1], v[2]);
-        double2 t2 = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
-        double2 t3 = cmul_si<S>(cscale(csub(v[1], v[2]), h));
+template <int S, typename C>
+struct Dft<3, S, C> {
+    __device__ __forceinline__ static void run(C* v, const double2*, int) {
+        using T = typename CplxT<C>::T;
+        const T h = (T)0.86602540378443864676;  // sqrt(3)/2
+        C t1 = cadd(v[1], v[2]);
+        C t2 = cmake<C>(v[0].x - (T)0.5 * t1.x, v[0].y - (T)0.5 * t1.y);
+        C t3 = cmul_si<S>(cscale(csub(v[1], v[2]), h));
         v[0] = cadd(v[0], t1);
         v[1] = cadd(t2, t3);
         v[2] = csub(t2, t3);
     }
 };
 
-template <int S>
-struct Dft<4, S> {
-    __device__ __forceinline__ static void run(double2* v, const double2*, int) {
-        double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-        double2 b0 = cadd(v[1], v[3]), b1 = cmul_si<S>(csub(v[1], v[3]));
+template <int S, typename C>
+struct Dft<4, S, C> {
+    __device__ __forceinline__ static void run(C* v, const double2*, int) {
+        C a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+        C b0 = cadd(v[1], v[3]), b1 = cmul_si<S>(csub(v[1], v[3]));
         v[0] = cadd(a0, b0);
         v[2] = csub(a0, b0);
         v[1] = cadd(a1, b1);
@@ -106,19 +137,20 @@ struct Dft<4, S> {
     }
 };
 
-template <int S>
-struct Dft<5, S> {
-    __device__ __forceinline__ static void run(double2* v, const double2*, int) {
-        const double c1 = 0.30901699437494742410;   // cos(2pi/5)
-        const double c2 = -0.80901699437494742410;  // cos(4pi/5)
-        const double s1 = 0.95105651629515357212;   // sin(2pi/5)
-        const double s2 = 0.58778525229247312917;   // sin(4pi/5)
-        double2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
-        double2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
-        double2 a1 = make_double2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
-        double2 a2 = make_double2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
-        double2 b1 = cmul_si<S>(make_double2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y));
-        double2 b2 = cmul_si<S>(make_double2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y));
+template <int S, typename C>
+struct Dft<5, S, C> {
+    __device__ __forceinline__ static void run(C* v, const double2*, int) {
+        using T = typename CplxT<C>::T;
+        const T c1 = (T)0.30901699437494742410;   // cos(2pi/5)
+        const T c2 = (T)-0.80901699437494742410;  // cos(4pi/5)
+        const T s1 = (T)0.95105651629515357212;   // sin(2pi/5)
+        const T s2 = (T)0.58778525229247312917;   // sin(4pi/5)
+        C t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        C t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        C a1 = cmake<C>(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+        C a2 = cmake<C>(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+        C b1 = cmul_si<S>(cmake<C>(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y));
+        C b2 = cmul_si<S>(cmake<C>(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y));
         v[0] = cadd(v[0], cadd(t1, t2));
         v[1] = cadd(a1, b1);
         v[4] = csub(a1, b1);
@@ -127,11 +159,12 @@ struct Dft<5, S> {
     }
 };
 
-template <int S>
-struct Dft<8, S> {
-    __device__ __forceinline__ static void run(double2* v, const double2*, int) {
-        const double r2 = 0.70710678118654752440;
-        double2 a[4], b[4];
+template <int S, typename C>
+struct Dft<8, S, C> {
+    __device__ __forceinline__ static void run(C* v, const double2*, int) {
+        using T = typename CplxT<C>::T;
+        const T r2 = (T)0.70710678118654752440;
+        C a[4], b[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             a[j] = cadd(v[j], v[j + 4]);
@@ -141,8 +174,8 @@ struct Dft<8, S> {
         b[1] = cscale(cadd(b[1], cmul_si<S>(b[1])), r2);
         b[2] = cmul_si<S>(b[2]);
         b[3] = cscale(csub(cmul_si<S>(b[3]), b[3]), r2);
-        Dft<4, S>::run(a, nullptr, 0);
-        Dft<4, S>::run(b, nullptr, 0);
+        Dft<4, S, C>::run(a, nullptr, 0);
+        Dft<4, S, C>::run(b, nullptr, 0);
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             v[2 * m] = a[m];
@@ -153,17 +186,17 @@ struct Dft<8, S> {
 
 // Generic odd radix (7) through the axis root table:
 // W_R^{m} = root[m * (n / R)] (conjugated for S = +1).
-template <int R, int S>
+template <int R, int S, typename C>
 struct DftGeneric {
-    __device__ __forceinline__ static void run(double2* v, const double2* root, int n) {
-        double2 y[R];
+    __device__ __forceinline__ static void run(C* v, const double2* root, int n) {
+        C y[R];
         const int step = n / R;
 #pragma unroll
         for (int d = 0; d < R; ++d) {
-            double2 s = v[0];
+            C s = v[0];
 #pragma unroll
             for (int b = 1; b < R; ++b) {
-                double2 w = __ldg(&root[((b * d) % R) * step]);
+                C w = ldroot<C>(&root[((b * d) % R) * step]);
                 if (S > 0) w.y = -w.y;
                 s = cadd(s, cmul(v[b], w));
             }
@@ -173,30 +206,30 @@ struct DftGeneric {
         for (int d = 0; d < R; ++d) v[d] = y[d];
     }
 };
-template <int S>
-struct Dft<7, S> : DftGeneric<7, S> {};
+template <int S, typename C>
+struct Dft<7, S, C> : DftGeneric<7, S, C> {};
 
 // Composite radix R = R1*R2 entirely in registers (four-step):
 //   y[k1 + R1 k2] = sum_n2 W_R2^{n2 k2} W_R^{n2 k1} sum_n1 x[R2 n1 + n2] W_R1^{n1 k1}
 // with W_R^m = root[m * (n / R)] (conjugated for S = +1).
-template <int R1, int R2, int S>
+template <int R1, int R2, int S, typename C>
 struct DftComposite {
-    __device__ __forceinline__ static void run(double2* v, const double2* root, int n) {
+    __device__ __forceinline__ static void run(C* v, const double2* root, int n) {
         constexpr int R = R1 * R2;
         const int step = n / R;
         // phase 1, in place: v[R2 k1 + n2] <- W_R^{n2 k1} DFT_R1(v[R2 n1 + n2])_k1
 #pragma unroll
         for (int n2 = 0; n2 < R2; ++n2) {
-            double2 u[R1];
+            C u[R1];
 #pragma unroll
             for (int n1 = 0; n1 < R1; ++n1) u[n1] = v[R2 * n1 + n2];
-            Dft<R1, S>::run(u, root, n);
+            Dft<R1, S, C>::run(u, root, n);
 #pragma unroll
             for (int k1 = 0; k1 < R1; ++k1) {
                 if (n2 * k1 == 0) {
                     v[R2 * k1 + n2] = u[k1];
                 } else {
-                    double2 w = __ldg(&root[n2 * k1 * step]);
+                    C w = ldroot<C>(&root[n2 * k1 * step]);
                     if (S > 0) w.y = -w.y;
                     v[R2 * k1 + n2] = cmul(u[k1], w);
                 }
@@ -204,9 +237,9 @@ struct DftComposite {
         }
         // phase 2, in place: v[R2 k1 + k2] <- DFT_R2(v[R2 k1 + n2])_k2
 #pragma unroll
-        for (int k1 = 0; k1 < R1; ++k1) Dft<R2, S>::run(v + R2 * k1, root, n);
+        for (int k1 = 0; k1 < R1; ++k1) Dft<R2, S, C>::run(v + R2 * k1, root, n);
         // y[k1 + R1 k2] = v[R2 k1 + k2]: a register permutation
-        double2 y[R];
+        C y[R];
 #pragma unroll
         for (int k1 = 0; k1 < R1; ++k1)
 #pragma unroll
@@ -215,19 +248,19 @@ struct DftComposite {
         for (int i = 0; i < R; ++i) v[i] = y[i];
     }
 };
-template <int S>
-struct Dft<6, S> : DftComposite<2, 3, S> {};
-template <int S>
-struct Dft<9, S> : DftComposite<3, 3, S> {};
-template <int S>
-struct Dft<10, S> : DftComposite<2, 5, S> {};
-template <int S>
-struct Dft<12, S> : DftComposite<4, 3, S> {};
+template <int S, typename C>
+struct Dft<6, S, C> : DftComposite<2, 3, S, C> {};
+template <int S, typename C>
+struct Dft<9, S, C> : DftComposite<3, 3, S, C> {};
+template <int S, typename C>
+struct Dft<10, S, C> : DftComposite<2, 5, S, C> {};
+template <int S, typename C>
+struct Dft<12, S, C> : DftComposite<4, 3, S, C> {};
 
 // One radix-R stage over every line of axis `ax` of the NBUF planes that
 // start at `buf[0]`, `buf[0] + bufstride`, ...  DIF when FWD, DIT otherwise.
-template <int R, bool FWD, int NBUF>
-__device__ __forceinline__ void stage_R(double2* buf, int bufstride, int Nk, const AxisPlan& ax, int s,
+template <int R, bool FWD, int NBUF, typename C>
+__device__ __forceinline__ void stage_R(C* buf, int bufstride, int Nk, const AxisPlan& ax, int s,
                                         const double2* __restrict__ root) {
     constexpr int S = FWD ? -1 : +1;
     const int n = ax.n;
@@ -249,16 +282,16 @@ __device__ __forceinline__ void stage_R(double2* buf, int bufstride, int Nk, con
         const int step = L * inner;
 #pragma unroll
         for (int q = 0; q < NBUF; ++q) {
-            double2* X = buf + q * bufstride;
-            double2 v[R];
+            C* X = buf + q * bufstride;
+            C v[R];
 #pragma unroll
             for (int b = 0; b < R; ++b) v[b] = X[base + b * step];
             if (FWD) {
-                Dft<R, S>::run(v, root, n);
+                Dft<R, S, C>::run(v, root, n);
                 if (a != 0) {
 #pragma unroll
                     for (int d = 1; d < R; ++d) {
-                        double2 w = __ldg(&root[a * d * tw_step]);
+                        const C w = ldroot<C>(&root[a * d * tw_step]);
                         v[d] = cmul(v[d], w);
                     }
                 }
@@ -266,12 +299,12 @@ __device__ __forceinline__ void stage_R(double2* buf, int bufstride, int Nk, con
                 if (a != 0) {
 #pragma unroll
                     for (int d = 1; d < R; ++d) {
-                        double2 w = __ldg(&root[a * d * tw_step]);
+                        C w = ldroot<C>(&root[a * d * tw_step]);
                         w.y = -w.y;
                         v[d] = cmul(v[d], w);
                     }
                 }
-                Dft<R, S>::run(v, root, n);
+                Dft<R, S, C>::run(v, root, n);
             }
 #pragma unroll
             for (int b = 0; b < R; ++b) X[base + b * step] = v[b];
@@ -284,14 +317,14 @@ constexpr int kRadixAll = (1 << 2) | (1 << 3) | (1 << 4) | (1 << 5) | (1 << 6) |
                           (1 << 10) | (1 << 12);
 constexpr int kRadix89 = (1 << 8) | (1 << 9);
 
-template <bool FWD, int NBUF, int MASK>
-__device__ __forceinline__ void run_stage(double2* buf, int bufstride, int Nk, const AxisPlan& ax, int s,
+template <bool FWD, int NBUF, int MASK, typename C>
+__device__ __forceinline__ void run_stage(C* buf, int bufstride, int Nk, const AxisPlan& ax, int s,
                                           const double2* __restrict__ roots) {
     const double2* root = roots + ax.rootoff;
     switch (ax.r[s]) {
-#define EDUS_STAGE_CASE(R)                                                                          \
-    case R:                                                                                         \
-        if constexpr ((MASK >> R) & 1) stage_R<R, FWD, NBUF>(buf, bufstride, Nk, ax, s, root);   \
+#define EDUS_STAGE_CASE(R)                                                                             \
+    case R:                                                                                            \
+        if constexpr ((MASK >> R) & 1) stage_R<R, FWD, NBUF, C>(buf, bufstride, Nk, ax, s, root);   \
         break;
         EDUS_STAGE_CASE(2)
         EDUS_STAGE_CASE(3)
@@ -309,28 +342,28 @@ __device__ __forceinline__ void run_stage(double2* buf, int bufstride, int Nk, c
 }
 
 // Forward (k -> R, unnormalised sign -1) transform of the plane(s) in place.
-template <int NBUF, int MASK>
-__device__ void plane_forward(double2* buf, int bufstride, const PlanePlan& pl, const double2* __restrict__ roots) {
+template <int NBUF, int MASK, typename C>
+__device__ void plane_forward(C* buf, int bufstride, const PlanePlan& pl, const double2* __restrict__ roots) {
 #pragma unroll 1
     for (int d = 0; d < 3; ++d) {
         const AxisPlan& ax = pl.ax[d];
 #pragma unroll 1
         for (int s = 0; s < ax.nst; ++s) {
-            run_stage<true, NBUF, MASK>(buf, bufstride, pl.Nk, ax, s, roots);
+            run_stage<true, NBUF, MASK, C>(buf, bufstride, pl.Nk, ax, s, roots);
             __syncthreads();
         }
     }
 }
 
 // Inverse (R -> k, unnormalised sign +1) transform, exact reverse of plane_forward.
-template <int NBUF, int MASK>
-__device__ void plane_inverse(double2* buf, int bufstride, const PlanePlan& pl, const double2* __restrict__ roots) {
+template <int NBUF, int MASK, typename C>
+__device__ void plane_inverse(C* buf, int bufstride, const PlanePlan& pl, const double2* __restrict__ roots) {
 #pragma unroll 1
     for (int d = 2; d >= 0; --d) {
         const AxisPlan& ax = pl.ax[d];
 #pragma unroll 1
         for (int s = ax.nst - 1; s >= 0; --s) {
-            run_stage<false, NBUF, MASK>(buf, bufstride, pl.Nk, ax, s, roots);
+            run_stage<false, NBUF, MASK, C>(buf, bufstride, pl.Nk, ax, s, roots);
             __syncthreads();
         }
     }

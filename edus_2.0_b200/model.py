@@ -328,10 +328,10 @@ class Model:
         self.hartree = hart
         self.DM0R = fft_k_to_R(self.rho0k, self.grid)
 
-    def solver(self, batch=1, device=0) -> "edus.Solver":
+    def solver(self, batch=1, device=0, precision=edus.PREC_FP64) -> "edus.Solver":
         cfg = self.cfg
         s = edus.Solver(self.grid, self.nb, cfg.dt, solver=cfg.solver, order=cfg.order, coulomb=cfg.coulomb,
-                        batch=batch, device=device)
+                        batch=batch, device=device, precision=precision)
         if cfg.coulomb:
             s.upload_model(self.H0k, self.xik, self.A, self.W, self.DM0R, self.hartree)
         else:

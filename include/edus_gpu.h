@@ -47,8 +47,29 @@ extern "C" {
 #define EDUS_SOLVER_AB 0
 #define EDUS_SOLVER_RK 1
 
-/* Arithmetic of the right-hand side.  FP64 is the drop-in form. */
+/* Forms of the right-hand side.
+ *   FP64   the drop-in form: every band pair, FP64 throughout, no assumption
+ *          on the symmetry of rho or H (as the reference).
+ *   HERM64 packed-Hermitian form: only band pairs n <= m are stored and
+ *          transformed, and the state is split rho = rho_ref + delta around
+ *          the first state set; all arithmetic FP64.  It propagates the
+ *          Hermitian part of the reference's generator.  The two are equal
+ *          on odd grids.  On an even axis the Gamma-centred index N/2 has
+ *          coordinate -N/2 for both R and -R, so the reference's gradient
+ *          i (R.E) rho(R) and its W_nm(R) there are not Hermitian-preserving.
+ *          Their Hermitian parts use coordinate 0 on that index and
+ *          (W_nm(R) + W_mn(-R)) / 2.  The difference grows with |rho(R)| on
+ *          the N/2 planes; the upload refuses a W that is asymmetric
+ *          anywhere else.  Diagonal f_nn are kept real.
+ *   MIXED  HERM64 with the per-step intermediates (gradient and self-energy
+ *          planes, the model planes, the RK stage input) stored and
+ *          transformed in FP32; the state delta, the RK accumulator, the AB
+ *          history and the constant terms of the split stay FP64, and the
+ *          band-matrix products run in FP64.
+ * HERM64 and MIXED need nbands <= 32. */
 #define EDUS_PREC_FP64 0
+#define EDUS_PREC_HERM64 1
+#define EDUS_PREC_MIXED 2
 
 /* Laser envelopes.  SIN2 is the reference's pulse (src/Laser/Laser.cpp:96-134):
  *   E(t) = sqrt(I) sin^2(pi (t-t0)/(cycles*T)) sin(w (t-t0) + phase) pol,
@@ -68,7 +89,7 @@ typedef struct {
     int order;       /* 4 for RK; 4 or 5 for AB */
     double dt;       /* DESolver::ResolutionTime, a.u. */
     int coulomb;     /* 1: add the HSEX self-energy (Coulomb::EffectiveHamiltonian) */
-    int precision;   /* EDUS_PREC_FP64 */
+    int precision;   /* EDUS_PREC_FP64, _HERM64 or _MIXED */
     int batch;       /* independent solves sharing one model (>= 1) */
     int device;      /* CUDA device ordinal */
 } edus_desc;

@@ -278,6 +278,12 @@ typedef struct {
     double r0_au[3];
     int nr0;               // number of r0 components given (1..3)
     int coulomb_fix_centres;  // 0 = reference behaviour (cumulative r), 1 = r = c_n - R - c_m
+    // 0 = reference behaviour.  1 = the Hermitian part of the generator on an
+    // even grid, where the Gamma-centred index N/2 sits at -N/2 for both R and
+    // -R: the gradient uses coordinate 0 there and W_nm(R) becomes
+    // (W_nm(R) + W_mn(-R)) / 2.  This is what the packed-Hermitian GPU forms
+    // propagate; it differs from the reference only on the N/2 planes.
+    int hermitian_nyquist;
     int nlasers;
     oracle_laser lasers[8];
 } oracle_cfg;
@@ -293,6 +299,7 @@ struct Sim {
     std::vector<cd> H0k, rk[3], H0R, rR[3];
     std::vector<double> Rcart;   // [Nk][3] Gamma-centred Cartesian R of FFT index
     std::vector<double> Rcrys;   // [Nk][3]
+    std::vector<double> Rgrad;   // [Nk][3] Cartesian R used by the k-gradient
     std::vector<double> eval;    // [Nk][nb]
     std::vector<cd> U;           // [Nk][nb][nb]
     std::vector<cd> vel[3];      // velocity operator in k
@@ -430,6 +437,17 @@ Sim* build(const oracle_cfg* cfg) {
         }
         for (int a = 0; a < 3; ++a) s.Rcart[3 * iR + a] = s.A[a][0] * c[0] + s.A[a][1] * c[1] + s.A[a][2] * c[2];
     }
+    s.Rgrad = s.Rcart;
+    if (cfg->hermitian_nyquist) {
+        for (int iR = 0; iR < Nk; ++iR) {
+            double c[3];
+            for (int d = 0; d < 3; ++d) {
+                c[d] = s.Rcrys[3 * iR + d];
+                if (s.N[d] % 2 == 0 && c[d] == -s.N[d] / 2.) c[d] = 0.;
+            }
+            for (int a = 0; a < 3; ++a) s.Rgrad[3 * iR + a] = s.A[a][0] * c[0] + s.A[a][1] * c[1] + s.A[a][2] * c[2];
+        }
+    }
     // lasers (Simulation.cpp:121-144, Laser.cpp)
     for (int il = 0; il < cfg->nlasers; ++il) {
         const oracle_laser& L = cfg->lasers[il];
@@ -530,6 +548,19 @@ Sim* build(const oracle_cfg* cfg) {
                 }
             }
         }
+        if (cfg->hermitian_nyquist) {
+            std::vector<cd> Ws(s.W);
+            for (int iR = 0; iR < Nk; ++iR) {
+                const int j[3] = {iR / (s.N[1] * s.N[2]), (iR / s.N[2]) % s.N[1], iR % s.N[2]};
+                const int mR = (((s.N[0] - j[0]) % s.N[0]) * s.N[1] + (s.N[1] - j[1]) % s.N[1]) * s.N[2] +
+                               (s.N[2] - j[2]) % s.N[2];
+                for (int n = 0; n < nb; ++n)
+                    for (int mm = 0; mm < nb; ++mm)
+                        Ws[((size_t)iR * nb + n) * nb + mm] =
+                            0.5 * (s.W[((size_t)iR * nb + n) * nb + mm] + s.W[((size_t)mR * nb + mm) * nb + n]);
+            }
+            s.W.swap(Ws);
+        }
         // Hartree_nm = sum_R V_nm(R), symmetrised (Coulomb.cpp:41-58)
         s.Hartree.assign(P, 0.);
         for (int iR = 0; iR < Nk; ++iR)
@@ -593,7 +624,7 @@ void source_term(Sim& s, cd* out_k, double time, const cd* in_k) {
     // kGradient R branch: out(R) += 1 * i (R.E) in(R)  (kGradient_definitions.hpp:35-40)
 #pragma omp parallel for schedule(static)
     for (int iR = 0; iR < s.Nk; ++iR) {
-        const double* Rc = &s.Rcart[3 * (size_t)iR];
+        const double* Rc = &s.Rgrad[3 * (size_t)iR];
         double dot = Rc[0] * E[0] + Rc[1] * E[1] + Rc[2] * E[2];
         for (int p = 0; p < P; ++p) s.outR[(size_t)iR * P + p] += (1. + 0. * im) * im * dot * s.inR[(size_t)iR * P + p];
     }

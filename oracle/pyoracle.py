@@ -111,6 +111,7 @@ class SimConfig:
     gradient_space: str
     lasers: list = field(default_factory=list)
     coulomb_fix_centres: bool = False
+    hermitian_nyquist: bool = False  # test switch: the packed forms' Hermitian generator
     printresolution: int = 1
     printresolution_pulse: int = 1
 
@@ -193,6 +194,7 @@ class _Cfg(ctypes.Structure):
                 ("solver", ctypes.c_int), ("order", ctypes.c_int), ("coulomb", ctypes.c_int),
                 ("epsilon", ctypes.c_double), ("r0_au", ctypes.c_double * 3),
                 ("nr0", ctypes.c_int), ("coulomb_fix_centres", ctypes.c_int),
+                ("hermitian_nyquist", ctypes.c_int),
                 ("nlasers", ctypes.c_int), ("lasers", _Laser * 8)]
 
 
@@ -258,6 +260,7 @@ def make_cfg(cfg: SimConfig) -> _Cfg:
         c.r0_au[i] = x
     c.nr0 = len(cfg.r0)
     c.coulomb_fix_centres = int(cfg.coulomb_fix_centres)
+    c.hermitian_nyquist = int(cfg.hermitian_nyquist)
     if len(cfg.lasers) > 8:
         raise ValueError("at most 8 lasers")
     c.nlasers = len(cfg.lasers)

@@ -221,6 +221,43 @@ def test_gradient_plane_wave_known_answer(po, pkg, tmp_path):
         assert np.abs(out - ana).max() < 1e-12 * max(1.0, np.abs(ana).max())
 
 
+def _hsex_cfg(po, pkg, tmp_path, grid, name):
+    uc, Rs, H, r = pkg.workloads.random_model(3, 5)
+    seed = os.path.join(str(tmp_path), name)
+    pkg.workloads.write_tb(seed + "_tb.dat", uc, Rs, H, r)
+    inp = pkg.workloads._input(seed, grid, 1, 0.01, 10, "RK",
+                               [pkg.workloads.gaussian_laser(1.5, 0.5, 0.02, 0.3, pol=(0.6, 1.0, 0.0))],
+                               coulomb=True, epsilon=2.0, r0_A=10.0)
+    return po.load_input(inp)
+
+
+def _herm_part_error(o, t, rho):
+    f = o.rhs(t, rho)
+    return np.abs(f - np.conj(np.transpose(f, (0, 2, 1)))).max() / np.abs(f).max()
+
+
+def test_hermitian_nyquist_switch(po, pkg, tmp_path):
+    """On an even grid the reference's generator (gradient at the Gamma-centred
+    index -N/2, and W there) is not Hermitian-preserving; the oracle's
+    hermitian_nyquist switch gives its Hermitian part, which the packed GPU
+    forms propagate.  On an odd grid the switch changes nothing."""
+    rng = np.random.default_rng(3)
+    t = 0.3 / 0.02418884326585747  # near the pulse centre, a.u.
+    for grid, even in (((6, 8, 1), True), ((7, 9, 1), False)):
+        cfg = _hsex_cfg(po, pkg, tmp_path, grid, "hn%d" % grid[0])
+        ref = po.Oracle(cfg)
+        cfg.hermitian_nyquist = True
+        herm = po.Oracle(cfg)
+        x = rng.normal(size=ref.shape) + 1j * rng.normal(size=ref.shape)
+        rho = ref.get("rho") + 0.05 * (x + np.conj(np.transpose(x, (0, 2, 1))))
+        assert _herm_part_error(herm, t, rho) < 1e-13
+        if even:
+            assert _herm_part_error(ref, t, rho) > 1e-6
+        else:
+            assert np.array_equal(ref.rhs(t, rho), herm.rhs(t, rho))
+            assert np.array_equal(ref.get("W"), herm.get("W"))
+
+
 @pytest.mark.skipif(not reference_available(), reason="reference sources not mounted")
 def test_hbn_generator_matches_reference_model(po, hbn_golden_model):
     import pyoracle
