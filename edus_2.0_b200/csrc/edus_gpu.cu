@@ -43,6 +43,10 @@ struct edus_handle {
     PlanePlan plan{};
     int smem_plane = 0, smem_comm = 0, TK = 4, comm_threads = 256;
     bool comm_mma = false;
+    // fused Hamiltonian (HSEX): sparse H0(R), xi_d(R) added in the plane kernel
+    int* hpos = nullptr;
+    double2* hval = nullptr;
+    int nS = 0;
     PlaneLaunch plane_cfg{0, 512, false};
     int plane_grid = 0;            // persistent plane kernel: CTAs per launch
     double2* plane_scratch = nullptr;  // [plane_grid][Nk]: rho(R) between the two inverse transforms
@@ -199,42 +203,45 @@ void prof_resolve(edus_handle* h) {
 
 template <bool COUL, int MASK, int MAXT>
 void launch_plane_variant(edus_handle* h, dim3 grid, const double2* in, long long in_bstride, double2* G,
-                          double2* Hee, long long out_bstride, const StageField* field) {
+                          double2* Hee, long long out_bstride, const StageField* field, int nS) {
     plane_rhs_kernel<COUL, MASK, MAXT><<<grid, h->plane_cfg.threads, h->smem_plane, h->stream>>>(
         in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
-        1.0 / h->Nk);
+        1.0 / h->Nk, h->hpos, h->hval, nS);
 }
 
 template <bool COUL, int MASK, int MAXT>
 void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long long in_bstride, double2* G,
-                          double2* Hee, long long out_bstride, const StageField* field) {
+                          double2* Hee, long long out_bstride, const StageField* field, int nS) {
     const int grid = std::min(nplanes, h->plane_grid);
     plane_rhs_persist_kernel<COUL, MASK, MAXT><<<grid, h->plane_cfg.threads, h->Nk * sizeof(double2), h->stream>>>(
         in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
-        1.0 / h->Nk, h->plane_scratch, nplanes);
+        1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS);
 }
 
+// fuse: with HSEX and a sparse model, Hee receives the whole Hamiltonian
+// H0 + E.xi + Hee (plane kernel) and the commutator reads only it.
 int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double2* G, double2* Hee,
-                 long long out_bstride, const StageField* field, int nbatch) {
+                 long long out_bstride, const StageField* field, int nbatch, bool fuse = true) {
     dim3 grid(h->P, nbatch);
     cudaEvent_t e0;
     prof_begin(h, &e0);
     const bool c = h->d.coulomb != 0;
+    const int nS = (fuse && c) ? h->nS : 0;
     if (h->plane_cfg.persist) {
         const int np = h->P * nbatch;
         if (h->plane_cfg.variant == 1) {
-            if (c) launch_plane_persist<true, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field);
-            else launch_plane_persist<false, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field);
+            if (c) launch_plane_persist<true, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
+            else launch_plane_persist<false, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
         } else {
-            if (c) launch_plane_persist<true, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field);
-            else launch_plane_persist<false, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field);
+            if (c) launch_plane_persist<true, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
+            else launch_plane_persist<false, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
         }
     } else if (h->plane_cfg.variant == 1) {
-        if (c) launch_plane_variant<true, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field);
-        else launch_plane_variant<false, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field);
+        if (c) launch_plane_variant<true, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field, nS);
+        else launch_plane_variant<false, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field, nS);
     } else {
-        if (c) launch_plane_variant<true, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field);
-        else launch_plane_variant<false, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field);
+        if (c) launch_plane_variant<true, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, nS);
+        else launch_plane_variant<false, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, nS);
     }
     h->launches++;
     CU(h, cudaGetLastError());
@@ -243,17 +250,22 @@ int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double
 }
 
 template <int MODE>
-int launch_comm_mode(edus_handle* h, const StageArgs& a, int nbatch) {
+int launch_comm_mode(edus_handle* h, const StageArgs& a, int nbatch, bool fuse) {
     dim3 grid((h->Nk + h->TK - 1) / h->TK, nbatch);
     cudaEvent_t e0;
     prof_begin(h, &e0);
+    const bool fh = fuse && h->d.coulomb && h->nS > 0;
     if (h->comm_mma) {
-        if (h->d.coulomb)
+        if (fh)
+            commutator_mma_kernel<MODE, true, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
+        else if (h->d.coulomb)
             commutator_mma_kernel<MODE, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
         else
             commutator_mma_kernel<MODE, false><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
     } else {
-        if (h->d.coulomb)
+        if (fh)
+            commutator_kernel<MODE, true, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
+        else if (h->d.coulomb)
             commutator_kernel<MODE, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
         else
             commutator_kernel<MODE, false><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
@@ -264,14 +276,14 @@ int launch_comm_mode(edus_handle* h, const StageArgs& a, int nbatch) {
     return EDUS_OK;
 }
 
-int launch_comm(edus_handle* h, int mode, const StageArgs& a, int nbatch) {
+int launch_comm(edus_handle* h, int mode, const StageArgs& a, int nbatch, bool fuse = true) {
     switch (mode) {
-        case MODE_RHS: return launch_comm_mode<MODE_RHS>(h, a, nbatch);
-        case MODE_RK1: return launch_comm_mode<MODE_RK1>(h, a, nbatch);
-        case MODE_RK2: return launch_comm_mode<MODE_RK2>(h, a, nbatch);
-        case MODE_RK3: return launch_comm_mode<MODE_RK3>(h, a, nbatch);
-        case MODE_RK4: return launch_comm_mode<MODE_RK4>(h, a, nbatch);
-        case MODE_AB: return launch_comm_mode<MODE_AB>(h, a, nbatch);
+        case MODE_RHS: return launch_comm_mode<MODE_RHS>(h, a, nbatch, fuse);
+        case MODE_RK1: return launch_comm_mode<MODE_RK1>(h, a, nbatch, fuse);
+        case MODE_RK2: return launch_comm_mode<MODE_RK2>(h, a, nbatch, fuse);
+        case MODE_RK3: return launch_comm_mode<MODE_RK3>(h, a, nbatch, fuse);
+        case MODE_RK4: return launch_comm_mode<MODE_RK4>(h, a, nbatch, fuse);
+        case MODE_AB: return launch_comm_mode<MODE_AB>(h, a, nbatch, fuse);
     }
     return fail(h, EDUS_ERR_ARG, "bad stage mode");
 }
@@ -422,6 +434,64 @@ int grid_for(long long n) { return (int)std::min<long long>((n + 255) / 256, 148
 
 // rho_ref := the full-plane state y[b]; C0, K_d, H0' from the FP64 full-plane
 // kernels, then packed (and rounded to the storage type).
+// H0(R) and xi_d(R) (k -> R transforms of the uploaded k arrays, as the
+// reference's go_to_R, Operator.hpp:566-586) on the lattice vectors where any
+// of them is non-zero, for the fused Hamiltonian of the HSEX plane kernel.
+// Entries below 1e-13 of an array's largest are transform rounding of zeros
+// and are dropped.  More than kMaxSparseR positions (a model dense in R): the
+// commutator assembles H from the k arrays instead.
+constexpr int kMaxSparseR = 4096;
+
+int build_sparse_model(edus_handle* h) {
+    h->nS = 0;
+    const int P = h->P, Nk = h->Nk;
+    const size_t S = h->S;
+    double2* tmp = nullptr;
+    CU(h, cudaMalloc((void**)&tmp, 4 * S * sizeof(double2)));
+    const double2* src[4] = {h->H0, h->xi[0], h->xi[1], h->xi[2]};
+    for (int a = 0; a < 4; ++a)
+        plane_to_R_kernel<kRadixAll, 256><<<P, 256, Nk * sizeof(double2), h->stream>>>(src[a], tmp + a * S, h->roots,
+                                                                                     h->plan, 1.0 / Nk);
+    h->launches += 4;
+    std::vector<double2> hv(4 * S);
+    const cudaError_t e1 = cudaGetLastError();
+    const cudaError_t e2 = cudaMemcpyAsync(hv.data(), tmp, 4 * S * sizeof(double2), cudaMemcpyDeviceToHost, h->stream);
+    const cudaError_t e3 = cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+        return fail(h, EDUS_ERR_CUDA, "k -> R transform of the model failed");
+    double mx[4] = {0, 0, 0, 0};
+    for (int a = 0; a < 4; ++a)
+        for (size_t i = 0; i < S; ++i) mx[a] = std::max(mx[a], std::hypot(hv[a * S + i].x, hv[a * S + i].y));
+    std::vector<int> pos;
+    for (int q = 0; q < Nk; ++q) {
+        bool keep = false;
+        for (int a = 0; a < 4 && !keep; ++a)
+            for (int p = 0; p < P && !keep; ++p) {
+                const double2 v = hv[a * S + (size_t)p * Nk + q];
+                keep = std::hypot(v.x, v.y) > 1e-13 * mx[a];
+            }
+        if (keep) pos.push_back(q);
+        if ((int)pos.size() > kMaxSparseR) return EDUS_OK;  // dense: unfused path
+    }
+    const int nS = (int)pos.size();
+    if (nS == 0) return EDUS_OK;
+    std::vector<double2> vals(4 * (size_t)P * nS);
+    for (int a = 0; a < 4; ++a)
+        for (int p = 0; p < P; ++p)
+            for (int s2 = 0; s2 < nS; ++s2) vals[((size_t)a * P + p) * nS + s2] = hv[a * S + (size_t)p * Nk + pos[s2]];
+    int rc;
+    if (!h->hpos) {
+        if ((rc = dalloc(h, (void**)&h->hpos, kMaxSparseR * sizeof(int)))) return rc;
+        if ((rc = dalloc(h, (void**)&h->hval, 4 * (size_t)P * kMaxSparseR * sizeof(double2)))) return rc;
+    }
+    CU(h, cudaMemcpyAsync(h->hpos, pos.data(), nS * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CU(h, cudaMemcpyAsync(h->hval, vals.data(), vals.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    h->nS = nS;
+    return EDUS_OK;
+}
+
 int fix_reference(edus_handle* h, int b) {
     int rc;
     const size_t Sb = h->S * sizeof(double2);
@@ -437,7 +507,7 @@ int fix_reference(edus_handle* h, int b) {
     }
     CU(h, cudaMemcpyAsync(h->ref_fields, rf, sizeof(rf), cudaMemcpyHostToDevice, h->stream));
     // E = 0: Hee(rho_ref), rho_ref diagonal at R = 0, then C0 = f(rho_ref; 0)
-    if ((rc = launch_plane(h, h->ref_full, 0, h->G, h->Hee, 0, h->ref_fields, 1))) return rc;
+    if ((rc = launch_plane(h, h->ref_full, 0, h->G, h->Hee, 0, h->ref_fields, 1, false))) return rc;
     const int coul = h->d.coulomb ? 1 : 0;
     const long long nS = (long long)h->S;
     assemble_h0p<<<grid_for(nS), 256, 0, h->stream>>>(h->H0, h->Hee, h->tmp_in, h->hartree, h->diag0, h->rho0diag,
@@ -447,15 +517,15 @@ int fix_reference(edus_handle* h, int b) {
     a.rho = h->ref_full;
     a.field = h->ref_fields;
     a.out = h->tmp_out;
-    if ((rc = launch_comm(h, MODE_RHS, a, 1))) return rc;  // tmp_out = C0 (full)
+    if ((rc = launch_comm(h, MODE_RHS, a, 1, false))) return rc;  // tmp_out = C0 (full)
     const long long nq = (long long)h->Sq;
     pack_planes<double2><<<grid_for(nq), 256, 0, h->stream>>>(h->tmp_out, h->pC0, h->qnm, h->nb, h->Pq, h->Nk);
     h->launches++;
     for (int d = 0; d < 3; ++d) {
-        if ((rc = launch_plane(h, h->ref_full, 0, h->G, h->Hee, 0, h->ref_fields + 1 + d, 1))) return rc;
+        if ((rc = launch_plane(h, h->ref_full, 0, h->G, h->Hee, 0, h->ref_fields + 1 + d, 1, false))) return rc;
         a.field = h->ref_fields + 1 + d;
         a.out = h->stage;
-        if ((rc = launch_comm(h, MODE_RHS, a, 1))) return rc;  // stage = f(rho_ref; e_d)
+        if ((rc = launch_comm(h, MODE_RHS, a, 1, false))) return rc;  // stage = f(rho_ref; e_d)
         sub_planes<<<grid_for(nS), 256, 0, h->stream>>>(h->stage, h->tmp_out, h->stage, nS);
         pack_planes<double2><<<grid_for(nq), 256, 0, h->stream>>>(h->stage, h->pK[d], h->qnm, h->nb, h->Pq, h->Nk);
         h->launches += 2;
@@ -608,11 +678,14 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     if ((rc = set_smem(h, plane_rhs_kernel<false, kRadixAll, 512>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_rhs_kernel<true, kRadix89, 768>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_rhs_kernel<false, kRadix89, 768>, h->smem_plane))) return bail(rc);
+    if ((rc = set_smem(h, plane_to_R_kernel<kRadixAll, 256>, h->Nk * (int)sizeof(double2)))) return bail(rc);
 #define SETC(M)                                                                                   \
     if ((rc = set_smem(h, commutator_kernel<M, true>, h->smem_comm))) return bail(rc);           \
     if ((rc = set_smem(h, commutator_kernel<M, false>, h->smem_comm))) return bail(rc);          \
     if ((rc = set_smem(h, commutator_mma_kernel<M, true>, h->smem_comm))) return bail(rc);       \
-    if ((rc = set_smem(h, commutator_mma_kernel<M, false>, h->smem_comm))) return bail(rc);
+    if ((rc = set_smem(h, commutator_mma_kernel<M, false>, h->smem_comm))) return bail(rc);     \
+    if ((rc = set_smem(h, commutator_kernel<M, true, true>, h->smem_comm))) return bail(rc);     \
+    if ((rc = set_smem(h, commutator_mma_kernel<M, true, true>, h->smem_comm))) return bail(rc);
     SETC(MODE_RHS) SETC(MODE_RK1) SETC(MODE_RK2) SETC(MODE_RK3) SETC(MODE_RK4) SETC(MODE_AB)
 #undef SETC
 
@@ -842,6 +915,7 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, co
         CU(h, cudaStreamSynchronize(h->stream));  // host vectors go out of scope
     }
     CU(h, cudaStreamSynchronize(h->stream));
+    if (h->d.coulomb && (rc = build_sparse_model(h))) return rc;
     if (h->packed) {
         // the packed forms need Hermitian H0, xi and W_nm(R) = W_mn(-R)
         const int nb = h->nb;

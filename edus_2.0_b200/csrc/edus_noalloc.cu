@@ -239,11 +239,11 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
     if (coulomb)
         plane_rhs_kernel<true, kRadixAll, 512><<<pg, 512, plane_smem, stream>>>(rho_pk, 0, G, Hee, 0, r0p, Wp, diag0,
                                                                                  d_field, d_roots, d_rpos, plan, nb,
-                                                                                 1.0 / Nk);
+                                                                                 1.0 / Nk, nullptr, nullptr, 0);
     else
         plane_rhs_kernel<false, kRadixAll, 512><<<pg, 512, plane_smem, stream>>>(rho_pk, 0, G, Hee, 0, r0p, Wp, diag0,
                                                                                   d_field, d_roots, d_rpos, plan, nb,
-                                                                                  1.0 / Nk);
+                                                                                  1.0 / Nk, nullptr, nullptr, 0);
     NA_CU(cudaGetLastError());
     StageArgs a{};
     a.rho = rho_pk;

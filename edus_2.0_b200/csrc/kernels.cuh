@@ -22,6 +22,48 @@ struct StageField {
     double g[3];
 };
 
+// Fused Hamiltonian (HSEX only): the model part H0(R) + sum_d E_d xi_d(R) is
+// added to the self-energy plane in R before its transform, as the reference
+// assembles H in R (Simulation.cpp:296-349), so the plane kernel returns
+// H_k = H0_k + E.xi_k + Hee_k and the commutator reads one Hamiltonian array.
+// H0(R) and xi(R) of a tight-binding model live on a few lattice vectors: nS
+// positions hpos[s] (digit-reversed plane order) with values
+// hval[(d * P + p) * nS + s], d = 0 for H0 and 1 + axis for xi.
+__device__ __forceinline__ void add_model_R(double2* X, const int* __restrict__ hpos,
+                                            const double2* __restrict__ hval, int nS, int p, int P,
+                                            const StageField& F) {
+    for (int s = threadIdx.x; s < nS; s += blockDim.x) {
+        double2 v = X[__ldg(&hpos[s])];
+        const double2 h0 = __ldg(&hval[(long long)p * nS + s]);
+        v.x += h0.x;
+        v.y += h0.y;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (F.E[d] != 0.0) {
+                const double2 x = __ldg(&hval[((long long)(d + 1) * P + p) * nS + s]);
+                v.x += F.E[d] * x.x;
+                v.y += F.E[d] * x.y;
+            }
+        }
+        X[__ldg(&hpos[s])] = v;
+    }
+}
+
+// k -> R transform of whole planes (set-up of the fused Hamiltonian):
+// dst[p][q] = FFT_{-1}(src[p])[q] / Nk in the digit-reversed position order q.
+template <int MASK, int MAXT>
+__global__ void __launch_bounds__(MAXT) plane_to_R_kernel(const double2* __restrict__ src, double2* __restrict__ dst,
+                                                          const double2* __restrict__ roots, PlanePlan pl,
+                                                          double inv_nk) {
+    extern __shared__ double2 smem[];
+    const int Nk = pl.Nk;
+    const long long off = (long long)blockIdx.x * Nk;
+    for (int i = threadIdx.x; i < Nk; i += blockDim.x) smem[i] = __ldg(&src[off + i]);
+    __syncthreads();
+    plane_forward<1, MASK>(smem, 0, pl, roots);
+    for (int i = threadIdx.x; i < Nk; i += blockDim.x) dst[off + i] = cscale(smem[i], inv_nk);
+}
+
 // ---------------------------------------------------------------------------
 // Plane kernel: one CTA per (band pair p, solve b).
 //   rho_R  = FFT_{-1}(rho_k) / Nk                      (Operator::go_to_R)
@@ -36,7 +78,8 @@ __global__ void __launch_bounds__(MAXT) plane_rhs_kernel(
     const double2* __restrict__ rho, long long batch_stride_in, double2* __restrict__ G_out,
     double2* __restrict__ Hee_out, long long batch_stride_out, const double2* __restrict__ rho0p,
     const double* __restrict__ Wp, double2* __restrict__ diag0, const StageField* __restrict__ field,
-    const double2* __restrict__ roots, const double* __restrict__ rpos, PlanePlan pl, int nb, double inv_nk) {
+    const double2* __restrict__ roots, const double* __restrict__ rpos, PlanePlan pl, int nb, double inv_nk,
+    const int* __restrict__ hpos, const double2* __restrict__ hval, int nS) {
     extern __shared__ double2 smem[];
     const int Nk = pl.Nk;
     double2* X = smem;
@@ -73,6 +116,10 @@ __global__ void __launch_bounds__(MAXT) plane_rhs_kernel(
         }
     }
     __syncthreads();
+    if (COUL && nS > 0) {
+        add_model_R(Y, hpos, hval, nS, p, nb * nb, F);
+        __syncthreads();
+    }
     // the two inverse transforms run one after the other (fewer live registers)
     plane_inverse<1, MASK>(X, 0, pl, roots);
     if (COUL) plane_inverse<1, MASK>(Y, 0, pl, roots);
@@ -99,7 +146,8 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     double2* __restrict__ Hee_out, long long batch_stride_out, const double2* __restrict__ rho0p,
     const double* __restrict__ Wp, double2* __restrict__ diag0, const StageField* __restrict__ field,
     const double2* __restrict__ roots, const double* __restrict__ rpos, PlanePlan pl, int nb, double inv_nk,
-    double2* __restrict__ scratch, int nplanes) {
+    double2* __restrict__ scratch, int nplanes, const int* __restrict__ hpos, const double2* __restrict__ hval,
+    int nS) {
     extern __shared__ double2 smem[];
     const int Nk = pl.Nk;
     const int P = nb * nb;
@@ -144,6 +192,10 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 X[j] = make_double2(-wv * (r.x - r0.x), -wv * (r.y - r0.y));
             }
             __syncthreads();
+            if (nS > 0) {
+                add_model_R(X, hpos, hval, nS, p, P, F);
+                __syncthreads();
+            }
             plane_inverse<1, MASK>(X, 0, pl, roots);
             double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
             for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = X[i];
@@ -258,14 +310,15 @@ __host__ __device__ inline CommGeom comm_geometry(int nb) {
 // (+ Hee + Hartree diagonal) and rho, element (p, kk) handed to store(i, j, kk, h, r).
 // Elements are taken U at a time with every global load issued before any is
 // used, so that each thread keeps several loads in flight.
-template <bool COUL, typename Store>
+template <bool COUL, bool FH, typename Store>
 __device__ __forceinline__ void load_stage_inputs(const StageArgs& a, const StageField& F, const double2* hh, int b,
                                                   int k0, Store store) {
     constexpr int U = 4;
     const int nb = a.nb, P = nb * nb, TK = a.TK, Nk = a.Nk;
     const long long boff = (long long)b * a.bstride;
     const int total = P * TK;
-    const bool e0 = F.E[0] != 0.0, e1 = F.E[1] != 0.0, e2 = F.E[2] != 0.0;
+    // with the fused Hamiltonian (FH) the Hee array already holds H0 + E.xi + Hee
+    const bool e0 = !FH && F.E[0] != 0.0, e1 = !FH && F.E[1] != 0.0, e2 = !FH && F.E[2] != 0.0;
     for (int base = threadIdx.x; base < total; base += U * blockDim.x) {
         double2 r[U], h[U], x0[U], x1[U], x2[U], he[U];
         long long el[U];
@@ -278,7 +331,7 @@ __device__ __forceinline__ void load_stage_inputs(const StageArgs& a, const Stag
             el[u] = (long long)p * Nk + k0 + kk;
             if (ok[u]) {
                 r[u] = __ldg(&a.rho[boff + el[u]]);
-                h[u] = __ldg(&a.H0[el[u]]);
+                if (!FH) h[u] = __ldg(&a.H0[el[u]]);
                 if (e0) x0[u] = __ldg(&a.xi[0][el[u]]);
                 if (e1) x1[u] = __ldg(&a.xi[1][el[u]]);
                 if (e2) x2[u] = __ldg(&a.xi[2][el[u]]);
@@ -293,7 +346,7 @@ __device__ __forceinline__ void load_stage_inputs(const StageArgs& a, const Stag
             const int i = p / nb, j = p - (p / nb) * nb;
             double2 hv = make_double2(0.0, 0.0), rv = make_double2(0.0, 0.0);
             if (ok[u]) {
-                hv = h[u];
+                hv = FH ? make_double2(0.0, 0.0) : h[u];
                 rv = r[u];
                 if (e0) { hv.x += F.E[0] * x0[u].x; hv.y += F.E[0] * x0[u].y; }
                 if (e1) { hv.x += F.E[1] * x1[u].x; hv.y += F.E[1] * x1[u].y; }
@@ -362,7 +415,7 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs& a, const double2
     }
 }
 
-template <int MODE, bool COUL>
+template <int MODE, bool COUL, bool FH = false>
 __global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
     extern __shared__ double2 sm[];
     const int nb = a.nb, TK = a.TK;
@@ -387,7 +440,7 @@ __global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
         }
         __syncthreads();
     }
-    load_stage_inputs<COUL>(a, F, hh, b, k0, [&](int i, int j, int kk, double2 h, double2 r) {
+    load_stage_inputs<COUL, FH>(a, F, hh, b, k0, [&](int i, int j, int kk, double2 h, double2 r) {
         const int o = kk * tile_stride + i * ld + j;
         Hs[o] = h;
         Rs[o] = r;
@@ -518,7 +571,7 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-template <int MODE, bool COUL>
+template <int MODE, bool COUL, bool FH = false>
 __global__ void __launch_bounds__(256, 2) commutator_mma_kernel(StageArgs a) {
     extern __shared__ double smd[];
     const int nb = a.nb, Nk = a.Nk;
@@ -544,7 +597,7 @@ __global__ void __launch_bounds__(256, 2) commutator_mma_kernel(StageArgs a) {
         }
     }
     __syncthreads();
-    load_stage_inputs<COUL>(a, F, hh, b, k0, [&](int i, int j, int kk, double2 h, double2 r) {
+    load_stage_inputs<COUL, FH>(a, F, hh, b, k0, [&](int i, int j, int kk, double2 h, double2 r) {
         double* T = tiles + (size_t)kk * 4 * mat + i * pitch + j;
         T[0] = h.x;
         T[mat] = h.y;
