@@ -207,8 +207,12 @@ def run_ours(args, rank, world, local_rank):
     plane_avg = plane_ms / max(plane_n, 1)
     comm_avg = comm_ms / max(comm_n, 1)
     peak, peak_kind = measured_peaks()
-    dominant = "plane_rhs_kernel" if plane_ms >= comm_ms else "commutator_kernel"
-    if dominant == "plane_rhs_kernel":
+    # the kernels this workload runs: the persistent plane kernel and, for
+    # HSEX with 12..24 bands, the TMA-fed commutator
+    plane_name = "plane_rhs_persist_kernel"
+    comm_name = "commutator_pipe_kernel" if (cfg.coulomb and 12 <= model.nb <= 24) else "commutator_mma_kernel"
+    dominant = plane_name if plane_ms >= comm_ms else comm_name
+    if dominant == plane_name:
         ach = plane_launch_B / (plane_avg / 1e3) / 1e9
     else:
         ach = comm_launch_B / (comm_avg / 1e3) / 1e9

@@ -15,6 +15,10 @@
 #include "../../include/edus_gpu.h"
 #include "kernels.cuh"
 #include "packed_kernels.cuh"
+#include "comm_pipe.cuh"
+#include <cudaTypedefs.h>
+#include <map>
+#include <mutex>
 #include "plane_plan.hpp"
 
 using namespace edus;
@@ -47,6 +51,11 @@ struct edus_handle {
     int* hpos = nullptr;
     double2* hval = nullptr;
     int nS = 0;
+    // pipelined commutator of the fused path (12 <= nb <= 24) and its
+    // tensor maps, one per (array, batch count)
+    bool comm_pipe = false;
+    int pipe_grid = 0;
+    std::map<std::pair<const void*, int>, CUtensorMap> tmaps;
     PlaneLaunch plane_cfg{0, 512, false};
     int plane_grid = 0;            // persistent plane kernel: CTAs per launch
     double2* plane_scratch = nullptr;  // [plane_grid][Nk]: rho(R) between the two inverse transforms
@@ -249,13 +258,73 @@ int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double
     return EDUS_OK;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda)
+PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+    });
+    return fn;
+}
+
+// The [nbatch][P][Nk] complex array at `base` as the 4-D tensor
+// {2 Nk, nb, nb, nbatch} of doubles, box {2 TK, nb, nb, 1}.
+const CUtensorMap* pipe_map(edus_handle* h, const void* base, int nbatch) {
+    const auto key = std::make_pair(base, nbatch);
+    auto it = h->tmaps.find(key);
+    if (it != h->tmaps.end()) return &it->second;
+    PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+    if (!enc) return nullptr;
+    const PipeGeom g = pipe_geometry(h->nb);
+    const cuuint64_t nb = (cuuint64_t)h->nb, Nk = (cuuint64_t)h->Nk;
+    const cuuint64_t dims[4] = {2 * Nk, nb, nb, (cuuint64_t)nbatch};
+    const cuuint64_t strides[3] = {Nk * 16, nb * Nk * 16, nb * nb * Nk * 16};
+    const cuuint32_t box[4] = {(cuuint32_t)(2 * g.TK), (cuuint32_t)nb, (cuuint32_t)nb, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUtensorMap m;
+    const CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return nullptr;
+    return &(h->tmaps[key] = m);
+}
+
+template <int MODE>
+int launch_pipe(edus_handle* h, const StageArgs& a, int nbatch) {
+    const PipeGeom g = pipe_geometry(h->nb);
+    const int ntiles = ((h->Nk + g.TK - 1) / g.TK) * nbatch;
+    const int grid = std::min(ntiles, h->pipe_grid);
+    PipeMaps maps;
+    const void* src[5] = {a.Hee, a.rho, a.G, a.y ? (const void*)a.y : (const void*)a.G,
+                          a.acc ? (const void*)a.acc : (const void*)a.G};
+    for (int i = 0; i < 5; ++i) {
+        const CUtensorMap* m = pipe_map(h, src[i], nbatch);
+        if (!m) return fail(h, EDUS_ERR_CUDA, "cuTensorMapEncodeTiled failed for a commutator operand");
+        maps.m[i] = *m;
+    }
+    if (g.tiles == 3)
+        commutator_pipe_kernel<MODE, 2, 576><<<grid, 576, g.smem, h->stream>>>(a, nbatch, maps, h->flag);
+    else
+        commutator_pipe_kernel<MODE, 2, 256><<<grid, 256, g.smem, h->stream>>>(a, nbatch, maps, h->flag);
+    return EDUS_OK;
+}
+
 template <int MODE>
 int launch_comm_mode(edus_handle* h, const StageArgs& a, int nbatch, bool fuse) {
     dim3 grid((h->Nk + h->TK - 1) / h->TK, nbatch);
     cudaEvent_t e0;
     prof_begin(h, &e0);
     const bool fh = fuse && h->d.coulomb && h->nS > 0;
-    if (h->comm_mma) {
+    if (fh && h->comm_pipe) {
+        int rc;
+        if ((rc = launch_pipe<MODE>(h, a, nbatch))) return rc;
+    } else if (h->comm_mma) {
         if (fh)
             commutator_mma_kernel<MODE, true, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
         else if (h->d.coulomb)
@@ -492,6 +561,15 @@ int build_sparse_model(edus_handle* h) {
     return EDUS_OK;
 }
 
+// Device status word: a bounded wait that ran out inside a kernel sets it.
+int check_status(edus_handle* h) {
+    int v = 0;
+    CU(h, cudaMemcpyAsync(&v, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    if (v) return fail(h, EDUS_ERR_TIMEOUT, "a bounded wait for tensor copies in the commutator ran out");
+    return EDUS_OK;
+}
+
 int fix_reference(edus_handle* h, int b) {
     int rc;
     const size_t Sb = h->S * sizeof(double2);
@@ -688,6 +766,27 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     if ((rc = set_smem(h, commutator_mma_kernel<M, true, true>, h->smem_comm))) return bail(rc);
     SETC(MODE_RHS) SETC(MODE_RK1) SETC(MODE_RK2) SETC(MODE_RK3) SETC(MODE_RK4) SETC(MODE_AB)
 #undef SETC
+    if (d.coulomb && pipe_supported(h->nb)) {
+        const PipeGeom pg = pipe_geometry(h->nb);
+        if ((int)pg.smem <= dev_smem) {
+#define SETP(M)                                                                                              \
+    if ((rc = set_smem(h, commutator_pipe_kernel<M, 2, 576>, (int)pg.smem))) return bail(rc);            \
+    if ((rc = set_smem(h, commutator_pipe_kernel<M, 2, 256>, (int)pg.smem))) return bail(rc);
+            SETP(MODE_RHS) SETP(MODE_RK1) SETP(MODE_RK2) SETP(MODE_RK3) SETP(MODE_RK4) SETP(MODE_AB)
+#undef SETP
+            int per_sm = 0;
+            if (pg.tiles == 3)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commutator_pipe_kernel<MODE_RK2, 2, 576>, 576, pg.smem);
+            else
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commutator_pipe_kernel<MODE_RK2, 2, 256>, 256, pg.smem);
+            int nsm = 0;
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d.device);
+            if (per_sm > 0 && nsm > 0 && tensor_map_encoder()) {
+                h->comm_pipe = true;
+                h->pipe_grid = per_sm * nsm;
+            }
+        }
+    }
 
     const size_t Sb = h->S * sizeof(double2);
     const size_t SBb = Sb * h->B;
@@ -730,6 +829,8 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     if (h->plane_cfg.persist && d.coulomb) TRY_ALLOC(h->plane_scratch, (size_t)h->plane_grid * h->Nk * sizeof(double2));
     TRY_ALLOC(h->popbuf, h->nb * sizeof(double));
     TRY_ALLOC(h->flag, sizeof(int));
+    if (cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream) != cudaSuccess)
+        return bail(fail(h, EDUS_ERR_CUDA, "cudaMemsetAsync failed"));
     if (d.precision != EDUS_PREC_FP64) {
         h->packed = true;
         h->mixed = d.precision == EDUS_PREC_MIXED;
@@ -1010,7 +1111,7 @@ int edus_get_state(edus_handle* h, int b, double* rho_k) {
     CU(h, cudaGetLastError());
     CU(h, cudaMemcpyAsync(rho_k, h->stage, h->S * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
     CU(h, cudaStreamSynchronize(h->stream));
-    return EDUS_OK;
+    return check_status(h);
 }
 
 int edus_set_time(edus_handle* h, double t) {
@@ -1056,7 +1157,7 @@ int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k) {
     CU(h, cudaGetLastError());
     CU(h, cudaMemcpyAsync(out_k, h->stage, h->S * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
     CU(h, cudaStreamSynchronize(h->stream));
-    return EDUS_OK;
+    return check_status(h);
 }
 
 int edus_step(edus_handle* h, int n) {
@@ -1168,7 +1269,7 @@ int edus_synchronize(edus_handle* h) {
     if (!h) return EDUS_ERR_ARG;
     CU(h, cudaSetDevice(h->d.device));
     CU(h, cudaStreamSynchronize(h->stream));
-    return EDUS_OK;
+    return check_status(h);
 }
 
 int edus_population_wannier(edus_handle* h, int b, double* pop) {
