@@ -16,6 +16,7 @@
 #include "kernels.cuh"
 #include "packed_kernels.cuh"
 #include "comm_pipe.cuh"
+#include "split_kernels.cuh"
 #include <cudaTypedefs.h>
 #include <map>
 #include <mutex>
@@ -56,6 +57,17 @@ struct edus_handle {
     bool comm_pipe = false;
     int pipe_grid = 0;
     std::map<std::pair<const void*, int>, CUtensorMap> tmaps;
+    // split-precision form (EDUS_PREC_SPLIT32): anchor rho_ref and its FP64 terms
+    bool split = false, anchored = false;
+    int anchor_every = 32, since_anchor = 0;
+    double2* sref = nullptr;
+    double2* sGref[3] = {nullptr, nullptr, nullptr};
+    double2* sHfix = nullptr;
+    double2* srefdiag0 = nullptr;
+    float* W32 = nullptr;
+    float2* split_scratch = nullptr;
+    StageField* unit_fields = nullptr;  // [3][B]: E = e_d
+    int split_grid = 0, split_threads = 256;
     PlaneLaunch plane_cfg{0, 512, false};
     int plane_grid = 0;            // persistent plane kernel: CTAs per launch
     double2* plane_scratch = nullptr;  // [plane_grid][Nk]: rho(R) between the two inverse transforms
@@ -229,11 +241,53 @@ void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long l
 
 // fuse: with HSEX and a sparse model, Hee receives the whole Hamiltonian
 // H0 + E.xi + Hee (plane kernel) and the commutator reads only it.
+int launch_split(edus_handle* h, const double2* in, double2* G, double2* H, const StageField* field, int nbatch) {
+    SplitArgs a{};
+    a.rho = in;
+    a.rref = h->sref;
+    a.bstride = (long long)h->S;
+    a.nplanes = h->P * nbatch;
+    a.G = G;
+    a.H = H;
+    for (int d = 0; d < 3; ++d) {
+        a.Gref[d] = h->sGref[d];
+        a.xi[d] = h->xi[d];
+    }
+    a.Hfix = h->sHfix;
+    a.W32 = h->W32;
+    a.refdiag0 = h->srefdiag0;
+    a.diag0 = h->diag0;
+    a.field = field;
+    a.roots = h->roots;
+    a.rpos = h->rpos;
+    a.scratch = h->split_scratch;
+    a.nb = h->nb;
+    a.inv_nk = 1.0 / h->Nk;
+    const int grid = std::min(a.nplanes, h->split_grid);
+    const size_t sm = (size_t)h->Nk * sizeof(float2);
+    const bool c = h->d.coulomb != 0;
+    if (h->plane_cfg.variant == 1) {
+        if (c) plane_split_kernel<true, kRadix89, 384><<<grid, h->split_threads, sm, h->stream>>>(a, h->plan);
+        else plane_split_kernel<false, kRadix89, 384><<<grid, h->split_threads, sm, h->stream>>>(a, h->plan);
+    } else {
+        if (c) plane_split_kernel<true, kRadixAll, 256><<<grid, h->split_threads, sm, h->stream>>>(a, h->plan);
+        else plane_split_kernel<false, kRadixAll, 256><<<grid, h->split_threads, sm, h->stream>>>(a, h->plan);
+    }
+    return EDUS_OK;
+}
+
 int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double2* G, double2* Hee,
                  long long out_bstride, const StageField* field, int nbatch, bool fuse = true) {
     dim3 grid(h->P, nbatch);
     cudaEvent_t e0;
     prof_begin(h, &e0);
+    if (h->split && fuse) {
+        launch_split(h, in, G, Hee, field, nbatch);
+        h->launches++;
+        CU(h, cudaGetLastError());
+        prof_end(h, 0, e0);
+        return EDUS_OK;
+    }
     const bool c = h->d.coulomb != 0;
     const int nS = (fuse && c) ? h->nS : 0;
     if (h->plane_cfg.persist) {
@@ -320,7 +374,7 @@ int launch_comm_mode(edus_handle* h, const StageArgs& a, int nbatch, bool fuse) 
     dim3 grid((h->Nk + h->TK - 1) / h->TK, nbatch);
     cudaEvent_t e0;
     prof_begin(h, &e0);
-    const bool fh = fuse && h->d.coulomb && h->nS > 0;
+    const bool fh = fuse && h->d.coulomb && (h->nS > 0 || h->split);
     if (fh && h->comm_pipe) {
         int rc;
         if ((rc = launch_pipe<MODE>(h, a, nbatch))) return rc;
@@ -561,6 +615,36 @@ int build_sparse_model(edus_handle* h) {
     return EDUS_OK;
 }
 
+// Split-precision anchor: rho_ref = the current state of every solve, and its
+// FP64 terms grad_d rho_ref (unit field along d), H0 + Hee(rho_ref) and
+// rho_ref,nn(R=0), by the FP64 plane kernel.
+int anchor_split(edus_handle* h) {
+    int rc;
+    const size_t SBb = h->S * sizeof(double2) * h->B;
+    const long long bs = (long long)h->S;
+    CU(h, cudaMemcpyAsync(h->sref, h->y, SBb, cudaMemcpyDeviceToDevice, h->stream));
+    const bool prof = h->profiling;
+    h->profiling = false;  // keep the anchor out of the per-kernel timings
+    for (int d = 0; d < 3; ++d) {
+        rc = launch_plane(h, h->sref, bs, h->sGref[d], h->Hee, bs, h->unit_fields + (size_t)d * h->B, h->B, false);
+        if (rc) {
+            h->profiling = prof;
+            return rc;
+        }
+        if (d == 0 && h->d.coulomb) {
+            add_broadcast_kernel<<<grid_for(bs * h->B), 256, 0, h->stream>>>(h->H0, h->Hee, h->sHfix, bs, h->B);
+            h->launches++;
+            CU(h, cudaMemcpyAsync(h->srefdiag0, h->diag0, (size_t)h->B * h->nb * sizeof(double2),
+                                  cudaMemcpyDeviceToDevice, h->stream));
+        }
+    }
+    h->profiling = prof;
+    CU(h, cudaGetLastError());
+    h->anchored = true;
+    h->since_anchor = 0;
+    return EDUS_OK;
+}
+
 // Device status word: a bounded wait that ran out inside a kernel sets it.
 int check_status(edus_handle* h) {
     int v = 0;
@@ -678,9 +762,11 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
         return fail(nullptr, EDUS_ERR_UNSUPPORTED, "RK is implemented for order 4 only (DESolver.hpp:157)");
     if (d.solver == EDUS_SOLVER_AB && d.order != 4 && d.order != 5)
         return fail(nullptr, EDUS_ERR_UNSUPPORTED, "order not implemented for AB (DESolver.hpp:120-124)");
-    if (d.precision != EDUS_PREC_FP64 && d.precision != EDUS_PREC_HERM64 && d.precision != EDUS_PREC_MIXED)
+    if (d.precision != EDUS_PREC_FP64 && d.precision != EDUS_PREC_HERM64 && d.precision != EDUS_PREC_MIXED &&
+        d.precision != EDUS_PREC_SPLIT32)
         return fail(nullptr, EDUS_ERR_UNSUPPORTED, "precision not supported");
-    if (d.precision != EDUS_PREC_FP64 && d.nbands > 32)
+    const bool packed_form = d.precision == EDUS_PREC_HERM64 || d.precision == EDUS_PREC_MIXED;
+    if (packed_form && d.nbands > 32)
         return fail(nullptr, EDUS_ERR_UNSUPPORTED, "the packed-Hermitian forms handle up to 32 bands");
     if (d.batch < 1) return fail(nullptr, EDUS_ERR_ARG, "batch must be >= 1");
     if (!(d.dt > 0.0) || !std::isfinite(d.dt)) return fail(nullptr, EDUS_ERR_ARG, "dt must be positive and finite");
@@ -712,7 +798,7 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     }
     const std::vector<double2>& roots = tabs.roots;
     std::vector<double>& rpos = tabs.rpos;
-    if (d.precision != EDUS_PREC_FP64) {
+    if (packed_form) {
         // The packed forms propagate the Hermitian part of the generator: on an
         // even axis the Gamma-centred index N/2 is -N/2 for both R and -R, so
         // the gradient's i (R.E) is not anti-Hermitian there; its Hermitian
@@ -831,7 +917,38 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     TRY_ALLOC(h->flag, sizeof(int));
     if (cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream) != cudaSuccess)
         return bail(fail(h, EDUS_ERR_CUDA, "cudaMemsetAsync failed"));
-    if (d.precision != EDUS_PREC_FP64) {
+    if (d.precision == EDUS_PREC_SPLIT32) {
+        h->split = true;
+        for (int dd = 0; dd < 3; ++dd) TRY_ALLOC(h->sGref[dd], SBb);
+        TRY_ALLOC(h->sref, SBb);
+        TRY_ALLOC(h->unit_fields, 3 * (size_t)h->B * sizeof(StageField));
+        if (d.coulomb) {
+            TRY_ALLOC(h->sHfix, SBb);
+            TRY_ALLOC(h->srefdiag0, (size_t)h->B * h->nb * sizeof(double2));
+            TRY_ALLOC(h->W32, (size_t)h->S * sizeof(float));
+        }
+        const size_t sm = (size_t)h->Nk * sizeof(float2);
+        if ((int)sm > dev_smem) return bail(fail(h, EDUS_ERR_UNSUPPORTED, "k grid too large for the split form"));
+        int per_sm = 0;
+        if (h->plane_cfg.variant == 1) {
+            h->split_threads = h->plane_cfg.persist ? h->plane_cfg.threads : 384;
+            if ((rc = set_smem(h, plane_split_kernel<true, kRadix89, 384>, (int)sm))) return bail(rc);
+            if ((rc = set_smem(h, plane_split_kernel<false, kRadix89, 384>, (int)sm))) return bail(rc);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plane_split_kernel<true, kRadix89, 384>,
+                                                          h->split_threads, sm);
+        } else {
+            h->split_threads = h->plane_cfg.persist ? h->plane_cfg.threads : 256;
+            if ((rc = set_smem(h, plane_split_kernel<true, kRadixAll, 256>, (int)sm))) return bail(rc);
+            if ((rc = set_smem(h, plane_split_kernel<false, kRadixAll, 256>, (int)sm))) return bail(rc);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plane_split_kernel<true, kRadixAll, 256>,
+                                                          h->split_threads, sm);
+        }
+        int nsm = 0;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d.device);
+        h->split_grid = std::max(1, per_sm) * std::max(1, nsm);
+        if (d.coulomb) TRY_ALLOC(h->split_scratch, (size_t)h->split_grid * h->Nk * sizeof(float2));
+    }
+    if (packed_form) {
         h->packed = true;
         h->mixed = d.precision == EDUS_PREC_MIXED;
         h->Pq = h->nb * (h->nb + 1) / 2;
@@ -1017,6 +1134,25 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, co
     }
     CU(h, cudaStreamSynchronize(h->stream));
     if (h->d.coulomb && (rc = build_sparse_model(h))) return rc;
+    if (h->split) {
+        // unit fields along x, y, z for the anchor's gradient terms; W in FP32
+        std::vector<StageField> uf(3 * (size_t)h->B);
+        for (int dd = 0; dd < 3; ++dd)
+            for (int b = 0; b < h->B; ++b) {
+                StageField& f = uf[(size_t)dd * h->B + b];
+                for (int i = 0; i < 3; ++i) f.E[i] = (i == dd) ? 1.0 : 0.0;
+                for (int c = 0; c < 3; ++c)
+                    f.g[c] = h->A[0 * 3 + c] * f.E[0] + h->A[1 * 3 + c] * f.E[1] + h->A[2 * 3 + c] * f.E[2];
+            }
+        CU(h, cudaMemcpyAsync(h->unit_fields, uf.data(), uf.size() * sizeof(StageField), cudaMemcpyHostToDevice,
+                              h->stream));
+        if (h->d.coulomb) {
+            to_float_kernel<<<grid_for((long long)h->S), 256, 0, h->stream>>>(h->Wp, h->W32, (long long)h->S);
+            h->launches++;
+        }
+        CU(h, cudaStreamSynchronize(h->stream));
+        h->anchored = false;
+    }
     if (h->packed) {
         // the packed forms need Hermitian H0, xi and W_nm(R) = W_mn(-R)
         const int nb = h->nb;
@@ -1093,6 +1229,7 @@ int edus_set_state(edus_handle* h, int b, const double* rho_k) {
         h->launches++;
         CU(h, cudaGetLastError());
     }
+    h->anchored = false;  // split form: the next step anchors at the new state
     CU(h, cudaStreamSynchronize(h->stream));
     return EDUS_OK;
 }
@@ -1130,6 +1267,10 @@ int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k) {
     if (!h || !in_k || !out_k) return EDUS_ERR_ARG;
     if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "edus_upload_model must be called first");
     CU(h, cudaSetDevice(h->d.device));
+    if (h->split && !h->anchored) {
+        int rc0;
+        if ((rc0 = anchor_split(h))) return rc0;
+    }
     int rc;
     if (!h->tmp_in) {
         if ((rc = dalloc(h, (void**)&h->tmp_in, h->S * sizeof(double2)))) return rc;
@@ -1226,6 +1367,10 @@ int edus_step(edus_handle* h, int n) {
             continue;
         }
         for (int i = 0; i < cnt; ++i) {
+            if (h->split && (!h->anchored || h->since_anchor >= h->anchor_every)) {
+                if ((rc = anchor_split(h))) return rc;
+            }
+            h->since_anchor++;
             const StageField* fs = h->field + (size_t)i * nst * B;
             StageArgs a = base_args(h);
             a.y = h->y;
@@ -1262,6 +1407,14 @@ int edus_step(edus_handle* h, int n) {
             h->t += dt;
         }
     }
+    return EDUS_OK;
+}
+
+int edus_set_anchor_interval(edus_handle* h, int steps) {
+    if (!h) return EDUS_ERR_ARG;
+    if (!h->split) return fail(h, EDUS_ERR_ARG, "the anchor interval belongs to the split-precision form");
+    if (steps < 1) return fail(h, EDUS_ERR_ARG, "the anchor interval must be >= 1 step");
+    h->anchor_every = steps;
     return EDUS_OK;
 }
 

@@ -24,7 +24,7 @@ EDUS_OK = 0
 ERRORS = {1: "EDUS_ERR_ARG", 2: "EDUS_ERR_CUDA", 3: "EDUS_ERR_TIMEOUT", 4: "EDUS_ERR_DIVERGED",
           5: "EDUS_ERR_UNSUPPORTED", 6: "EDUS_ERR_NOMEM"}
 SOLVER_AB, SOLVER_RK = 0, 1
-PREC_FP64, PREC_HERM64, PREC_MIXED = 0, 1, 2
+PREC_FP64, PREC_HERM64, PREC_MIXED, PREC_SPLIT32 = 0, 1, 2, 3
 ENVELOPE_SIN2, ENVELOPE_GAUSS = 0, 1
 
 # every entry point of include/edus_gpu.h
@@ -33,6 +33,7 @@ EXPORTS = [
     "edus_set_state", "edus_get_state", "edus_set_time", "edus_get_time", "edus_rhs", "edus_step",
     "edus_synchronize", "edus_population_wannier", "edus_device_bytes", "edus_kernel_launches",
     "edus_get_stream", "edus_set_profiling", "edus_get_profile", "edus_rhs_noalloc",
+    "edus_set_anchor_interval",
 ]
 
 
@@ -105,6 +106,7 @@ def load_library(path: str | None = None):
     L.edus_set_profiling.argtypes = [h, ctypes.c_int]
     L.edus_get_profile.argtypes = [h, ctypes.c_int, dp, P(ctypes.c_ulonglong)]
     vp = ctypes.c_void_p
+    L.edus_set_anchor_interval.argtypes = [h, ctypes.c_int]
     L.edus_rhs_noalloc.argtypes = [P(ctypes.c_int), ctypes.c_int, ctypes.c_int, dp, dp, vp, vp, vp, vp, vp, vp, vp,
                                    vp, ctypes.c_char_p, ctypes.c_int]
     for name in EXPORTS:
@@ -252,6 +254,10 @@ class Solver:
 
     def synchronize(self):
         self._check(self._L.edus_synchronize(self._h))
+
+    def set_anchor_interval(self, steps):
+        """Split-precision form: steps between moves of the anchor rho_ref."""
+        self._check(self._L.edus_set_anchor_interval(self._h, int(steps)))
 
     def population_wannier(self, b=0):
         out = np.empty(self.nb)

@@ -70,6 +70,16 @@ extern "C" {
 #define EDUS_PREC_FP64 0
 #define EDUS_PREC_HERM64 1
 #define EDUS_PREC_MIXED 2
+/*   SPLIT32 the full generator of FP64 (every band pair, the reference's own
+ *          gradient and self-energy on every grid) with the state split as
+ *          rho = rho_ref + delta.  The terms of rho_ref (grad rho_ref,
+ *          H0 + Hee(rho_ref), rho_ref,nn(R=0)) are FP64, computed when the
+ *          anchor rho_ref is moved to the current state: at the first step,
+ *          after edus_set_state and every edus_set_anchor_interval steps
+ *          (default 32).  Only delta goes through the plane transforms, in
+ *          FP32, so their rounding scales with |delta|.  The commutator, the
+ *          stage updates and the state are FP64. */
+#define EDUS_PREC_SPLIT32 3
 
 /* Laser envelopes.  SIN2 is the reference's pulse (src/Laser/Laser.cpp:96-134):
  *   E(t) = sqrt(I) sin^2(pi (t-t0)/(cycles*T)) sin(w (t-t0) + phase) pol,
@@ -89,7 +99,7 @@ typedef struct {
     int order;       /* 4 for RK; 4 or 5 for AB */
     double dt;       /* DESolver::ResolutionTime, a.u. */
     int coulomb;     /* 1: add the HSEX self-energy (Coulomb::EffectiveHamiltonian) */
-    int precision;   /* EDUS_PREC_FP64, _HERM64 or _MIXED */
+    int precision;   /* EDUS_PREC_FP64, _HERM64, _MIXED or _SPLIT32 */
     int batch;       /* independent solves sharing one model (>= 1) */
     int device;      /* CUDA device ordinal */
 } edus_desc;
@@ -154,6 +164,10 @@ int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k);
 /* Advance every solve by n steps (DESolver::Propagate(n), DESolver.hpp:238-242).
  * Asynchronous: returns once the work is queued. */
 int edus_step(edus_handle* h, int n);
+
+/* Split-precision form: steps between two moves of the anchor rho_ref to the
+ * current state (>= 1; default 32).  No reference counterpart. */
+int edus_set_anchor_interval(edus_handle* h, int steps);
 
 /* Wait for queued work; reports device-side errors. */
 int edus_synchronize(edus_handle* h);
