@@ -52,6 +52,12 @@ struct edus_handle {
     int* hpos = nullptr;
     double2* hval = nullptr;
     int nS = 0;
+    // Fock term given by the caller on nO lattice vectors (edus_set_fock_override)
+    int* opos = nullptr;
+    double2* oval = nullptr;
+    int nO = 0, nO_cap = 0;
+    // position (digit-reversed plane order) of each frequency index, per axis
+    std::vector<int> posof[3];
     // pipelined commutator of the fused path (12 <= nb <= 24) and its
     // tensor maps, one per (array, batch count)
     bool comm_pipe = false;
@@ -236,7 +242,7 @@ void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long l
     const int grid = std::min(nplanes, h->plane_grid);
     plane_rhs_persist_kernel<COUL, MASK, MAXT><<<grid, h->plane_cfg.threads, h->Nk * sizeof(double2), h->stream>>>(
         in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
-        1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS);
+        1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0);
 }
 
 // fuse: with HSEX and a sparse model, Hee receives the whole Hamiltonian
@@ -645,6 +651,22 @@ int anchor_split(edus_handle* h) {
     return EDUS_OK;
 }
 
+// plane position (digit-reversed order) of the natural R index (j0 N1 + j1) N2 + j2
+int position_of(const edus_handle* h, int iR) {
+    const int j2 = iR % h->N[2], j1 = (iR / h->N[2]) % h->N[1], j0 = iR / (h->N[1] * h->N[2]);
+    return (h->posof[0][j0] * h->N[1] + h->posof[1][j1]) * h->N[2] + h->posof[2][j2];
+}
+
+// out[s][p] = planes[p][pos[s]]
+__global__ void gather_R_kernel(const double2* __restrict__ planes, const int* __restrict__ pos, int nsel, int P,
+                                int Nk, double2* __restrict__ out) {
+    const long long total = (long long)nsel * P;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(i / P), p = (int)(i - (long long)s * P);
+        out[i] = planes[(long long)p * Nk + pos[s]];
+    }
+}
+
 // Device status word: a bounded wait that ran out inside a kernel sets it.
 int check_status(edus_handle* h) {
     int v = 0;
@@ -795,6 +817,10 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     {
         std::string perr;
         if (!build_plane_plan(h->N, h->plan, tabs, perr)) return bail(fail(h, EDUS_ERR_UNSUPPORTED, perr));
+    }
+    for (int ax = 0; ax < 3; ++ax) {
+        h->posof[ax].assign(h->N[ax], 0);
+        for (int q = 0; q < h->N[ax]; ++q) h->posof[ax][tabs.fq[tabs.fqoff[ax] + q]] = q;
     }
     const std::vector<double2>& roots = tabs.roots;
     std::vector<double>& rpos = tabs.rpos;
@@ -1407,6 +1433,81 @@ int edus_step(edus_handle* h, int n) {
             h->t += dt;
         }
     }
+    return EDUS_OK;
+}
+
+int edus_state_rspace(edus_handle* h, int b, int nsel, const int* R_index, double* out) {
+    if (!h || nsel < 0 || (nsel > 0 && (!R_index || !out))) return EDUS_ERR_ARG;
+    if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
+    if (nsel == 0) return EDUS_OK;
+    CU(h, cudaSetDevice(h->d.device));
+    int rc;
+    if (h->packed && (rc = unpack_state(h, b))) return rc;
+    std::vector<int> pos(nsel);
+    for (int s = 0; s < nsel; ++s) {
+        if (R_index[s] < 0 || R_index[s] >= h->Nk) return fail(h, EDUS_ERR_ARG, "R index out of range");
+        pos[s] = position_of(h, R_index[s]);
+    }
+    double2* tmp = nullptr;
+    int* dpos = nullptr;
+    double2* dout = nullptr;
+    CU(h, cudaMalloc((void**)&tmp, h->S * sizeof(double2)));
+    if (cudaMalloc((void**)&dpos, nsel * sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void**)&dout, (size_t)nsel * h->P * sizeof(double2)) != cudaSuccess) {
+        cudaFree(tmp);
+        cudaFree(dpos);
+        return fail(h, EDUS_ERR_NOMEM, "edus_state_rspace: allocation failed");
+    }
+    plane_to_R_kernel<kRadixAll, 256><<<h->P, 256, h->Nk * sizeof(double2), h->stream>>>(
+        h->y + (size_t)b * h->S, tmp, h->roots, h->plan, 1.0 / h->Nk);
+    cudaMemcpyAsync(dpos, pos.data(), nsel * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    gather_R_kernel<<<grid_for((long long)nsel * h->P), 256, 0, h->stream>>>(tmp, dpos, nsel, h->P, h->Nk, dout);
+    h->launches += 2;
+    cudaMemcpyAsync(out, dout, (size_t)nsel * h->P * sizeof(double2), cudaMemcpyDeviceToHost, h->stream);
+    const cudaError_t e = cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    cudaFree(dpos);
+    cudaFree(dout);
+    if (e != cudaSuccess) return fail(h, EDUS_ERR_CUDA, std::string("edus_state_rspace: ") + cudaGetErrorString(e));
+    return EDUS_OK;
+}
+
+int edus_set_fock_override(edus_handle* h, int nsel, const int* R_index, const double* values) {
+    if (!h || nsel < 0 || (nsel > 0 && (!R_index || !values))) return EDUS_ERR_ARG;
+    if (nsel == 0) {
+        if (h->nO) {
+            CU(h, cudaStreamSynchronize(h->stream));
+            h->nO = 0;
+        }
+        return EDUS_OK;
+    }
+    if (!h->d.coulomb || h->packed || h->split || !h->plane_cfg.persist)
+        return fail(h, EDUS_ERR_UNSUPPORTED,
+                    "a given Fock term needs the FP64 form with HSEX and a plane that fits two CTAs per SM");
+    if (nsel > h->Nk) return fail(h, EDUS_ERR_ARG, "more lattice vectors than grid points");
+    CU(h, cudaSetDevice(h->d.device));
+    std::vector<int> pos(nsel);
+    for (int s = 0; s < nsel; ++s) {
+        if (R_index[s] < 0 || R_index[s] >= h->Nk) return fail(h, EDUS_ERR_ARG, "R index out of range");
+        pos[s] = position_of(h, R_index[s]);
+    }
+    // values [nsel][nb][nb] -> [p][nsel]
+    std::vector<double2> v((size_t)h->P * nsel);
+    for (int s = 0; s < nsel; ++s)
+        for (int p = 0; p < h->P; ++p)
+            v[(size_t)p * nsel + s] =
+                make_double2(values[2 * ((size_t)s * h->P + p)], values[2 * ((size_t)s * h->P + p) + 1]);
+    CU(h, cudaStreamSynchronize(h->stream));  // kernels in flight may still read the previous values
+    int rc;
+    if (nsel > h->nO_cap) {
+        if ((rc = dalloc(h, (void**)&h->opos, nsel * sizeof(int)))) return rc;
+        if ((rc = dalloc(h, (void**)&h->oval, (size_t)h->P * nsel * sizeof(double2)))) return rc;
+        h->nO_cap = nsel;
+    }
+    CU(h, cudaMemcpyAsync(h->opos, pos.data(), nsel * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CU(h, cudaMemcpyAsync(h->oval, v.data(), v.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    h->nO = nsel;
     return EDUS_OK;
 }
 

@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     const double* __restrict__ Wp, double2* __restrict__ diag0, const StageField* __restrict__ field,
     const double2* __restrict__ roots, const double* __restrict__ rpos, PlanePlan pl, int nb, double inv_nk,
     double2* __restrict__ scratch, int nplanes, const int* __restrict__ hpos, const double2* __restrict__ hval,
-    int nS) {
+    int nS, const int* __restrict__ opos, const double2* __restrict__ oval, int nO) {
     extern __shared__ double2 smem[];
     const int Nk = pl.Nk;
     const int P = nb * nb;
@@ -183,13 +183,21 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
         for (int i = threadIdx.x; i < Nk; i += blockDim.x) gdst[i] = X[i];
         if (COUL) {
             __syncthreads();  // the stores above read X before it is refilled
-            const double2* r0p = rho0p + (long long)p * Nk;
-            const double* wp = Wp + (long long)p * Nk;
-            for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
-                const double2 r = slot[j];
-                const double2 r0 = __ldg(&r0p[j]);
-                const double wv = __ldg(&wp[j]);
-                X[j] = make_double2(-wv * (r.x - r0.x), -wv * (r.y - r0.y));
+            if (nO > 0) {
+                // the Fock term is given (values on nO lattice vectors, zero elsewhere)
+                for (int j = threadIdx.x; j < Nk; j += blockDim.x) X[j] = make_double2(0.0, 0.0);
+                __syncthreads();
+                for (int s2 = threadIdx.x; s2 < nO; s2 += blockDim.x)
+                    X[__ldg(&opos[s2])] = __ldg(&oval[(long long)p * nO + s2]);
+            } else {
+                const double2* r0p = rho0p + (long long)p * Nk;
+                const double* wp = Wp + (long long)p * Nk;
+                for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
+                    const double2 r = slot[j];
+                    const double2 r0 = __ldg(&r0p[j]);
+                    const double wv = __ldg(&wp[j]);
+                    X[j] = make_double2(-wv * (r.x - r0.x), -wv * (r.y - r0.y));
+                }
             }
             __syncthreads();
             if (nS > 0) {

@@ -33,7 +33,9 @@ EXPORTS = [
     "edus_set_state", "edus_get_state", "edus_set_time", "edus_get_time", "edus_rhs", "edus_step",
     "edus_synchronize", "edus_population_wannier", "edus_device_bytes", "edus_kernel_launches",
     "edus_get_stream", "edus_set_profiling", "edus_get_profile", "edus_rhs_noalloc",
-    "edus_set_anchor_interval",
+    "edus_set_anchor_interval", "edus_state_rspace", "edus_set_fock_override",
+    "edus_mlp_create", "edus_mlp_destroy", "edus_mlp_last_error", "edus_mlp_param_count", "edus_mlp_set_params",
+    "edus_mlp_get_params", "edus_mlp_forward", "edus_mlp_gradients", "edus_mlp_train_step",
 ]
 
 
@@ -107,10 +109,26 @@ def load_library(path: str | None = None):
     L.edus_get_profile.argtypes = [h, ctypes.c_int, dp, P(ctypes.c_ulonglong)]
     vp = ctypes.c_void_p
     L.edus_set_anchor_interval.argtypes = [h, ctypes.c_int]
+    ip = P(ctypes.c_int)
+    L.edus_state_rspace.argtypes = [h, ctypes.c_int, ctypes.c_int, ip, dp]
+    L.edus_set_fock_override.argtypes = [h, ctypes.c_int, ip, dp]
+    mp = ctypes.c_void_p
+    fp = P(ctypes.c_float)
+    L.edus_mlp_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong, ctypes.c_int, P(mp)]
+    L.edus_mlp_destroy.argtypes = [mp]
+    L.edus_mlp_last_error.argtypes = [mp]
+    L.edus_mlp_last_error.restype = ctypes.c_char_p
+    L.edus_mlp_param_count.argtypes = [mp]
+    L.edus_mlp_param_count.restype = ctypes.c_longlong
+    L.edus_mlp_set_params.argtypes = [mp, fp]
+    L.edus_mlp_get_params.argtypes = [mp, fp]
+    L.edus_mlp_forward.argtypes = [mp, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    L.edus_mlp_gradients.argtypes = [mp, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, fp, fp]
+    L.edus_mlp_train_step.argtypes = [mp, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, fp]
     L.edus_rhs_noalloc.argtypes = [P(ctypes.c_int), ctypes.c_int, ctypes.c_int, dp, dp, vp, vp, vp, vp, vp, vp, vp,
                                    vp, ctypes.c_char_p, ctypes.c_int]
     for name in EXPORTS:
-        if name != "edus_last_error":
+        if name not in ("edus_last_error", "edus_mlp_last_error", "edus_mlp_param_count"):
             getattr(L, name).restype = ctypes.c_int
     if path is None:
         _lib = L

@@ -165,6 +165,39 @@ int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k);
  * Asynchronous: returns once the work is queued. */
 int edus_step(edus_handle* h, int n);
 
+/* rho(R) of solve b at nsel lattice vectors: out[s][n][m] = rho_nm(R_s) with
+ * rho(R) = FFT_{-1}(rho_k) / Nk (Operator::go_to_R, Operator.hpp:566-586) and
+ * R_index[s] the natural R index (j0 N1 + j1) N2 + j2.  Synchronous.  No
+ * reference counterpart (inputs and training data of the learned self-energy). */
+int edus_state_rspace(edus_handle* h, int b, int nsel, const int* R_index, double* out);
+
+/* Replace the Fock term -W (rho(R) - rho0(R)) of every following right-hand
+ * side by given values on nsel lattice vectors (values[s][n][m] complex, zero
+ * elsewhere); the Hartree term stays exact.  nsel = 0 restores the exact term.
+ * FP64 form with HSEX whose plane fits two CTAs per SM.  No reference
+ * counterpart (the learned self-energy feeds the propagation through it). */
+int edus_set_fock_override(edus_handle* h, int nsel, const int* R_index, const double* values);
+
+/* Learned self-energy network: a multilayer perceptron n_in -> 3 hidden layers
+ * of n_hidden (GELU) -> n_out, BF16 weights with FP32 master copies and FP32
+ * accumulation, trained on the GPU (mean squared error, Adam).  Batches are
+ * row-major [batch][features] FP32 DEVICE buffers.  Parameters are flattened
+ * as W0 b0 W1 b1 W2 b2 W3 b3, W_l row-major [in][out] (host FP32 buffers).
+ * No reference counterpart. */
+typedef struct edus_mlp edus_mlp;
+int edus_mlp_create(int n_in, int n_hidden, int n_out, unsigned long long seed, int device, edus_mlp** out);
+int edus_mlp_destroy(edus_mlp* m);
+const char* edus_mlp_last_error(const edus_mlp* m);
+long long edus_mlp_param_count(const edus_mlp* m);
+int edus_mlp_set_params(edus_mlp* m, const float* host);
+int edus_mlp_get_params(edus_mlp* m, float* host);
+int edus_mlp_forward(edus_mlp* m, int batch, const float* x, float* y);
+/* loss and the gradient of every parameter (host buffers; either may be NULL) */
+int edus_mlp_gradients(edus_mlp* m, int batch, const float* x, const float* target, float* grads_host,
+                       float* loss_host);
+/* one Adam step on the batch; loss_host (may be NULL) receives the loss before the step */
+int edus_mlp_train_step(edus_mlp* m, int batch, const float* x, const float* target, float lr, float* loss_host);
+
 /* Split-precision form: steps between two moves of the anchor rho_ref to the
  * current state (>= 1; default 32).  No reference counterpart. */
 int edus_set_anchor_interval(edus_handle* h, int steps);
