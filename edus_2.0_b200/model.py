@@ -283,6 +283,7 @@ class Model:
         if not iorg:
             raise ValueError("model has no R=0 block")
         wc = np.array([[r[d, iorg[0], n, n].real for d in range(3)] for n in range(nb)])
+        self.centres = wc  # [nb][3] Wannier centres (bohr)
         md, mdn = np.array([100.0, 0.0, 0.0]), 100.0
         for n in range(nb):
             for m in range(n + 1, nb):
