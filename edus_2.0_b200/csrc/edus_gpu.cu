@@ -52,6 +52,10 @@ struct edus_handle {
     int* hpos = nullptr;
     double2* hval = nullptr;
     int nS = 0;
+    // a model (H0, xi) per solve (edus_upload_model_solve): [B][P][Nk] each
+    bool per_solve = false;
+    double2* H0b = nullptr;
+    double2* xib[3] = {nullptr, nullptr, nullptr};
     // Fock term given by the caller on nO lattice vectors (edus_set_fock_override)
     int* opos = nullptr;
     double2* oval = nullptr;
@@ -425,8 +429,9 @@ int set_smem(edus_handle* h, K kernel, int bytes) {
 
 StageArgs base_args(edus_handle* h) {
     StageArgs a{};
-    a.H0 = h->H0;
-    for (int d = 0; d < 3; ++d) a.xi[d] = h->xi[d];
+    a.H0 = h->per_solve ? h->H0b : h->H0;
+    for (int d = 0; d < 3; ++d) a.xi[d] = h->per_solve ? h->xib[d] : h->xi[d];
+    a.mstride = h->per_solve ? (long long)h->S : 0;
     a.Hee = h->Hee;
     a.G = h->G;
     a.hartree = h->hartree;
@@ -869,13 +874,15 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     if ((rc = set_smem(h, plane_rhs_kernel<true, kRadix89, 768>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_rhs_kernel<false, kRadix89, 768>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_to_R_kernel<kRadixAll, 256>, h->Nk * (int)sizeof(double2)))) return bail(rc);
+    // the attribute covers both commutator variants, which the autotuner may swap
+    const int smem_cmax = (int)std::max(comm_geometry(h->nb).smem, mma_geometry(h->nb).smem);
 #define SETC(M)                                                                                   \
-    if ((rc = set_smem(h, commutator_kernel<M, true>, h->smem_comm))) return bail(rc);           \
-    if ((rc = set_smem(h, commutator_kernel<M, false>, h->smem_comm))) return bail(rc);          \
-    if ((rc = set_smem(h, commutator_mma_kernel<M, true>, h->smem_comm))) return bail(rc);       \
-    if ((rc = set_smem(h, commutator_mma_kernel<M, false>, h->smem_comm))) return bail(rc);     \
-    if ((rc = set_smem(h, commutator_kernel<M, true, true>, h->smem_comm))) return bail(rc);     \
-    if ((rc = set_smem(h, commutator_mma_kernel<M, true, true>, h->smem_comm))) return bail(rc);
+    if ((rc = set_smem(h, commutator_kernel<M, true>, smem_cmax))) return bail(rc);           \
+    if ((rc = set_smem(h, commutator_kernel<M, false>, smem_cmax))) return bail(rc);          \
+    if ((rc = set_smem(h, commutator_mma_kernel<M, true>, smem_cmax))) return bail(rc);       \
+    if ((rc = set_smem(h, commutator_mma_kernel<M, false>, smem_cmax))) return bail(rc);     \
+    if ((rc = set_smem(h, commutator_kernel<M, true, true>, smem_cmax))) return bail(rc);     \
+    if ((rc = set_smem(h, commutator_mma_kernel<M, true, true>, smem_cmax))) return bail(rc);
     SETC(MODE_RHS) SETC(MODE_RK1) SETC(MODE_RK2) SETC(MODE_RK3) SETC(MODE_RK4) SETC(MODE_AB)
 #undef SETC
     if (d.coulomb && pipe_supported(h->nb)) {
@@ -1219,6 +1226,43 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, co
     return EDUS_OK;
 }
 
+int edus_upload_model_solve(edus_handle* h, int b, const double* H0_k, const double* xi_k) {
+    if (!h || !H0_k || !xi_k) return EDUS_ERR_ARG;
+    if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
+    if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "edus_upload_model (lattice and shared model) must come first");
+    if (h->d.coulomb || h->packed || h->split)
+        return fail(h, EDUS_ERR_UNSUPPORTED, "a model per solve is implemented for the FP64 form without HSEX");
+    CU(h, cudaSetDevice(h->d.device));
+    const size_t Sb = h->S * sizeof(double2);
+    int rc;
+    if (!h->per_solve) {
+        // every solve starts from the shared model
+        if ((rc = dalloc(h, (void**)&h->H0b, Sb * h->B))) return rc;
+        for (int d = 0; d < 3; ++d)
+            if ((rc = dalloc(h, (void**)&h->xib[d], Sb * h->B))) return rc;
+        for (int q = 0; q < h->B; ++q) {
+            CU(h, cudaMemcpyAsync(h->H0b + (size_t)q * h->S, h->H0, Sb, cudaMemcpyDeviceToDevice, h->stream));
+            for (int d = 0; d < 3; ++d)
+                CU(h, cudaMemcpyAsync(h->xib[d] + (size_t)q * h->S, h->xi[d], Sb, cudaMemcpyDeviceToDevice,
+                                      h->stream));
+        }
+        h->per_solve = true;
+    }
+    dim3 tb(32, 8), tg((h->Nk + 31) / 32, (h->P + 31) / 32);
+    auto up = [&](const double* src, double2* dst) -> int {
+        CU(h, cudaMemcpyAsync(h->stage, src, Sb, cudaMemcpyHostToDevice, h->stream));
+        transpose_kp_to_pk<<<tg, tb, 0, h->stream>>>(h->stage, dst, h->Nk, h->P);
+        h->launches++;
+        CU(h, cudaGetLastError());
+        return EDUS_OK;
+    };
+    if ((rc = up(H0_k, h->H0b + (size_t)b * h->S))) return rc;
+    for (int d = 0; d < 3; ++d)
+        if ((rc = up(xi_k + 2 * h->S * d, h->xib[d] + (size_t)b * h->S))) return rc;
+    CU(h, cudaStreamSynchronize(h->stream));  // the host buffers are the caller's
+    return EDUS_OK;
+}
+
 int edus_set_lasers(edus_handle* h, int b, int n, const edus_laser* lasers) {
     if (!h) return EDUS_ERR_ARG;
     if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
@@ -1327,6 +1371,74 @@ int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k) {
     return check_status(h);
 }
 
+// Host field table of `cnt` steps from the handle's time: stage times as
+// DESolver uses them, CurrentTime accumulated by += dt (DESolver.hpp:167-186,
+// 205-219); tab[(i * stages + s) * B + b].
+static void fill_field_table(edus_handle* h, int cnt, StageField* tab) {
+    const int nst = h->d.solver == EDUS_SOLVER_RK ? 4 : 1;
+    const double dt = h->d.dt;
+    double t = h->t;
+    for (int i = 0; i < cnt; ++i) {
+        double ts[4] = {t, t + dt / 2., t + dt / 2., t + dt};
+        for (int s = 0; s < nst; ++s)
+            for (int b = 0; b < h->B; ++b) field_at(h->lasers[b], h->A, ts[s], tab[((size_t)i * nst + s) * h->B + b]);
+        t += dt;
+    }
+}
+
+// Kernels of `cnt` steps of the full-matrix forms (FP64, SPLIT32) on the
+// handle's stream, the field table of those steps being in h->field; advances
+// the handle's time and AB ring.
+static int launch_plain_steps(edus_handle* h, int cnt) {
+    const bool rk = h->d.solver == EDUS_SOLVER_RK;
+    const int nst = rk ? 4 : 1;
+    const double dt = h->d.dt;
+    const int B = h->B;
+    const long long bs = (long long)h->S;
+    int rc;
+    for (int i = 0; i < cnt; ++i) {
+        if (h->split && (!h->anchored || h->since_anchor >= h->anchor_every)) {
+            if ((rc = anchor_split(h))) return rc;
+        }
+        h->since_anchor++;
+        const StageField* fs = h->field + (size_t)i * nst * B;
+        StageArgs a = base_args(h);
+        a.y = h->y;
+        if (rk) {
+            a.aux = h->aux;
+            a.acc = h->acc;
+            const double c0[4] = {dt / 2., dt / 2., dt, dt / 6.};
+            const double c1[4] = {dt / 6., dt / 3., dt / 3., 0.};
+            for (int s = 0; s < 4; ++s) {
+                const double2* in = (s == 0) ? h->y : h->aux;
+                if ((rc = launch_plane(h, in, bs, h->G, h->Hee, bs, fs + (size_t)s * B, B))) return rc;
+                a.rho = in;
+                a.field = fs + (size_t)s * B;
+                a.c[0] = c0[s];
+                a.c[1] = c1[s];
+                if ((rc = launch_comm(h, MODE_RK1 + s, a, B))) return rc;
+            }
+        } else {
+            if ((rc = launch_plane(h, h->y, bs, h->G, h->Hee, bs, fs, B))) return rc;
+            a.rho = h->y;
+            a.field = fs;
+            a.order = h->d.order;
+            for (int q = 0; q < h->d.order; ++q) {
+                a.hist[q] = h->hist[h->index[q]];
+                a.c[q] = dt * h->beta[q];
+            }
+            if ((rc = launch_comm(h, MODE_AB, a, B))) return rc;
+            // rotate the ring (DESolver.hpp:212-217)
+            const int ord = h->d.order;
+            int tmp = h->index[ord - 1];
+            for (int q = ord - 1; q > 0; --q) h->index[q] = h->index[q - 1];
+            h->index[0] = tmp;
+        }
+        h->t += dt;
+    }
+    return EDUS_OK;
+}
+
 int edus_step(edus_handle* h, int n) {
     if (!h || n < 0) return EDUS_ERR_ARG;
     if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "edus_upload_model must be called first");
@@ -1335,7 +1447,6 @@ int edus_step(edus_handle* h, int n) {
     const int nst = rk ? 4 : 1;
     const double dt = h->d.dt;
     const int B = h->B;
-    const long long bs = (long long)h->S;
     int rc;
     for (int s0 = 0; s0 < n; s0 += h->chunk) {
         const int cnt = std::min(h->chunk, n - s0);
@@ -1345,13 +1456,7 @@ int edus_step(edus_handle* h, int n) {
         h->field_cur ^= 1;
         CU(h, cudaEventSynchronize(h->field_ev[buf]));
         StageField* tab = h->field_host[buf];
-        double t = h->t;
-        for (int i = 0; i < cnt; ++i) {
-            double ts[4] = {t, t + dt / 2., t + dt / 2., t + dt};
-            for (int s = 0; s < nst; ++s)
-                for (int b = 0; b < B; ++b) field_at(h->lasers[b], h->A, ts[s], tab[((size_t)i * nst + s) * B + b]);
-            t += dt;
-        }
+        fill_field_table(h, cnt, tab);
         // the device table of the previous chunk is no longer read once the
         // kernels before this copy (same stream) have run
         CU(h, cudaMemcpyAsync(h->field, tab, (size_t)cnt * nst * B * sizeof(StageField), cudaMemcpyHostToDevice, h->stream));
@@ -1392,48 +1497,229 @@ int edus_step(edus_handle* h, int n) {
             }
             continue;
         }
-        for (int i = 0; i < cnt; ++i) {
-            if (h->split && (!h->anchored || h->since_anchor >= h->anchor_every)) {
-                if ((rc = anchor_split(h))) return rc;
-            }
-            h->since_anchor++;
-            const StageField* fs = h->field + (size_t)i * nst * B;
-            StageArgs a = base_args(h);
-            a.y = h->y;
-            if (rk) {
-                a.aux = h->aux;
-                a.acc = h->acc;
-                const double c0[4] = {dt / 2., dt / 2., dt, dt / 6.};
-                const double c1[4] = {dt / 6., dt / 3., dt / 3., 0.};
-                for (int s = 0; s < 4; ++s) {
-                    const double2* in = (s == 0) ? h->y : h->aux;
-                    if ((rc = launch_plane(h, in, bs, h->G, h->Hee, bs, fs + (size_t)s * B, B))) return rc;
-                    a.rho = in;
-                    a.field = fs + (size_t)s * B;
-                    a.c[0] = c0[s];
-                    a.c[1] = c1[s];
-                    if ((rc = launch_comm(h, MODE_RK1 + s, a, B))) return rc;
-                }
-            } else {
-                if ((rc = launch_plane(h, h->y, bs, h->G, h->Hee, bs, fs, B))) return rc;
-                a.rho = h->y;
-                a.field = fs;
-                a.order = h->d.order;
-                for (int q = 0; q < h->d.order; ++q) {
-                    a.hist[q] = h->hist[h->index[q]];
-                    a.c[q] = dt * h->beta[q];
-                }
-                if ((rc = launch_comm(h, MODE_AB, a, B))) return rc;
-                // rotate the ring (DESolver.hpp:212-217)
-                const int ord = h->d.order;
-                int tmp = h->index[ord - 1];
-                for (int q = ord - 1; q > 0; --q) h->index[q] = h->index[q - 1];
-                h->index[0] = tmp;
-            }
-            h->t += dt;
-        }
+        if ((rc = launch_plain_steps(h, cnt))) return rc;
     }
     return EDUS_OK;
+}
+
+int edus_sweep_step(edus_handle* const* hs, int n, int steps, int use_graph) {
+    if (!hs || n < 1 || steps < 0) return EDUS_ERR_ARG;
+    for (int i = 0; i < n; ++i)
+        if (!hs[i]) return EDUS_ERR_ARG;
+    edus_handle* h0 = hs[0];
+    bool graph = use_graph != 0;
+    for (int i = 0; i < n; ++i) {
+        edus_handle* h = hs[i];
+        if (h->d.device != h0->d.device) return fail(h0, EDUS_ERR_ARG, "a sweep's handles share one device");
+        if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "edus_upload_model must be called first");
+        if (h->packed || h->split)
+            return fail(h, EDUS_ERR_UNSUPPORTED, "a sweep steps the FP64 form (step other forms with edus_step)");
+        for (int j = 0; j < i; ++j)
+            if (hs[j] == h) return fail(h, EDUS_ERR_ARG, "a handle appears twice in the sweep");
+        if (h->d.solver != EDUS_SOLVER_RK || h->profiling) graph = false;
+    }
+    if (steps == 0) return EDUS_OK;
+    CU(h0, cudaSetDevice(h0->d.device));
+    constexpr int C = 32;  // steps per captured chunk (<= the field-table capacity)
+    cudaStream_t s0 = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join(n, nullptr);
+    cudaGraphExec_t exec = nullptr;
+    int rc = EDUS_OK;
+    auto cleanup = [&]() {
+        if (s0) cudaStreamSynchronize(s0);
+        if (exec) cudaGraphExecDestroy(exec);
+        for (auto& e : join)
+            if (e) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (s0) cudaStreamDestroy(s0);
+    };
+    if (cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) != cudaSuccess) {
+        cleanup();
+        return fail(h0, EDUS_ERR_CUDA, "sweep stream/event creation failed");
+    }
+    for (auto& e : join)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            cleanup();
+            return fail(h0, EDUS_ERR_CUDA, "sweep event creation failed");
+        }
+    // every handle's launches of `cnt` steps, forked from and joined into s0
+    auto launch_all = [&](int cnt) -> int {
+        if (cudaEventRecord(fork, s0) != cudaSuccess) return fail(h0, EDUS_ERR_CUDA, "cudaEventRecord failed");
+        for (int i = 0; i < n; ++i) {
+            edus_handle* h = hs[i];
+            if (cudaStreamWaitEvent(h->stream, fork, 0) != cudaSuccess)
+                return fail(h, EDUS_ERR_CUDA, "cudaStreamWaitEvent failed");
+            int r;
+            if ((r = launch_plain_steps(h, cnt))) return r;
+            if (cudaEventRecord(join[i], h->stream) != cudaSuccess || cudaStreamWaitEvent(s0, join[i], 0) != cudaSuccess)
+                return fail(h, EDUS_ERR_CUDA, "sweep join failed");
+        }
+        return EDUS_OK;
+    };
+    for (int done = 0; done < steps && rc == EDUS_OK;) {
+        const int cnt = std::min(C, steps - done);
+        // field tables of the chunk, uploaded on s0 ahead of the chunk's kernels
+        for (int i = 0; i < n && rc == EDUS_OK; ++i) {
+            edus_handle* h = hs[i];
+            const int nst = h->d.solver == EDUS_SOLVER_RK ? 4 : 1;
+            const int buf = h->field_cur;
+            h->field_cur ^= 1;
+            if (cudaEventSynchronize(h->field_ev[buf]) != cudaSuccess) rc = fail(h, EDUS_ERR_CUDA, "event sync failed");
+            StageField* tab = h->field_host[buf];
+            fill_field_table(h, cnt, tab);
+            if (rc == EDUS_OK &&
+                (cudaMemcpyAsync(h->field, tab, (size_t)cnt * nst * h->B * sizeof(StageField), cudaMemcpyHostToDevice,
+                                 s0) != cudaSuccess ||
+                 cudaEventRecord(h->field_ev[buf], s0) != cudaSuccess))
+                rc = fail(h, EDUS_ERR_CUDA, "field table upload failed");
+        }
+        if (rc) break;
+        if (graph && cnt == C) {
+            if (!exec) {
+                // capture one chunk of every handle once; replays reuse it (the
+                // kernels read the field table from the same device buffers)
+                std::vector<double> t0(n);
+                std::vector<unsigned long long> l0(n);
+                for (int i = 0; i < n; ++i) {
+                    t0[i] = hs[i]->t;
+                    l0[i] = hs[i]->launches;
+                }
+                cudaGraph_t g = nullptr;
+                if (cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                    rc = fail(h0, EDUS_ERR_CUDA, "cudaStreamBeginCapture failed");
+                    break;
+                }
+                const int r = launch_all(C);
+                const cudaError_t ec = cudaStreamEndCapture(s0, &g);
+                for (int i = 0; i < n; ++i) {  // the capture ran nothing
+                    hs[i]->t = t0[i];
+                    hs[i]->launches = l0[i];
+                }
+                if (r || ec != cudaSuccess || cudaGraphInstantiate(&exec, g, 0) != cudaSuccess) {
+                    if (g) cudaGraphDestroy(g);
+                    rc = r ? r : fail(h0, EDUS_ERR_CUDA, "capture of the sweep chunk failed");
+                    break;
+                }
+                cudaGraphDestroy(g);
+            }
+            if (cudaGraphLaunch(exec, s0) != cudaSuccess) {
+                rc = fail(h0, EDUS_ERR_CUDA, "cudaGraphLaunch failed");
+                break;
+            }
+            for (int i = 0; i < n; ++i) {
+                for (int k = 0; k < C; ++k) hs[i]->t += hs[i]->d.dt;  // as the launches would
+                hs[i]->launches += 8LL * C;
+            }
+        } else {
+            rc = launch_all(cnt);
+        }
+        done += cnt;
+    }
+    cleanup();
+    if (rc) return rc;
+    for (int i = 0; i < n; ++i)
+        if ((rc = check_status(hs[i]))) return rc;
+    return EDUS_OK;
+}
+
+int edus_autotune(edus_handle* h, int* plane_threads, int* comm_tensor) {
+    if (!h) return EDUS_ERR_ARG;
+    if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "edus_upload_model must be called first");
+    if (h->packed) return fail(h, EDUS_ERR_UNSUPPORTED, "the packed forms have their own launch geometry");
+    CU(h, cudaSetDevice(h->d.device));
+    CU(h, cudaStreamSynchronize(h->stream));
+    // a field along every axis, on every solve, for the timed launches
+    std::vector<StageField> f(h->B);
+    for (auto& x : f) {
+        for (int i = 0; i < 3; ++i) x.E[i] = 1e-3;
+        for (int c = 0; c < 3; ++c) x.g[c] = 1e-3 * (h->A[0 * 3 + c] + h->A[1 * 3 + c] + h->A[2 * 3 + c]);
+    }
+    StageField* df = nullptr;
+    CU(h, cudaMalloc((void**)&df, f.size() * sizeof(StageField)));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const bool prof = h->profiling;
+    h->profiling = false;
+    int rc = EDUS_OK;
+    const long long bs = (long long)h->S;
+    auto time_it = [&](auto&& launch) -> float {
+        for (int w = 0; w < 2; ++w) launch();
+        cudaEventRecord(e0, h->stream);
+        for (int r = 0; r < 5; ++r) launch();
+        cudaEventRecord(e1, h->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms;
+    };
+    cudaMemcpy(df, f.data(), f.size() * sizeof(StageField), cudaMemcpyHostToDevice);
+    // plane kernel: thread counts, multiples of 32 up to the variant's maximum
+    {
+        const int tmax = h->plane_cfg.persist ? (h->plane_cfg.variant == 1 ? 384 : 256)
+                                              : (h->plane_cfg.variant == 1 ? 768 : 512);
+        const int keep = h->plane_cfg.threads;
+        int best_t = keep;
+        float best = 1e30f;
+        for (int T = 128; T <= tmax; T += 32) {
+            h->plane_cfg.threads = T;
+            if (h->split) h->split_threads = T;
+            const float ms = time_it([&] { launch_plane(h, h->y, bs, h->G, h->Hee, bs, df, h->B); });
+            if (cudaGetLastError() != cudaSuccess) continue;
+            if (ms < best) {
+                best = ms;
+                best_t = T;
+            }
+        }
+        h->plane_cfg.threads = best_t;
+        if (h->split) h->split_threads = best_t;
+        if (plane_threads) *plane_threads = best_t;
+    }
+    // commutator: the CUDA-core against the tensor-core kernel (the TMA kernel
+    // of the fused HSEX path has one geometry)
+    {
+        const bool fused = h->d.coulomb && (h->nS > 0 || h->split) && h->comm_pipe;
+        if (!fused) {
+            StageArgs a = base_args(h);
+            a.rho = h->y;
+            a.field = df;
+            a.out = h->stage;
+            float best = 1e30f;
+            bool best_mma = h->comm_mma;
+            for (int mma = 0; mma < 2; ++mma) {
+                const CommGeom cg = comm_geometry(h->nb);
+                const MmaGeom mg = mma_geometry(h->nb);
+                h->comm_mma = mma != 0;
+                h->TK = mma ? mg.TK : cg.TK;
+                h->comm_threads = mma ? 256 : cg.threads;
+                h->smem_comm = (int)(mma ? mg.smem : cg.smem);
+                a.TK = h->TK;
+                const float ms = time_it([&] { launch_comm(h, MODE_RHS, a, 1); });
+                if (cudaGetLastError() != cudaSuccess) continue;
+                if (ms < best) {
+                    best = ms;
+                    best_mma = mma != 0;
+                }
+            }
+            const CommGeom cg = comm_geometry(h->nb);
+            const MmaGeom mg = mma_geometry(h->nb);
+            h->comm_mma = best_mma;
+            h->TK = best_mma ? mg.TK : cg.TK;
+            h->comm_threads = best_mma ? 256 : cg.threads;
+            h->smem_comm = (int)(best_mma ? mg.smem : cg.smem);
+        }
+        if (comm_tensor) *comm_tensor = h->comm_mma ? 1 : 0;
+    }
+    h->profiling = prof;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const cudaError_t e = cudaStreamSynchronize(h->stream);
+    cudaFree(df);
+    if (e != cudaSuccess) rc = fail(h, EDUS_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+    if (rc == EDUS_OK) rc = check_status(h);
+    return rc;
 }
 
 int edus_state_rspace(edus_handle* h, int b, int nsel, const int* R_index, double* out) {

@@ -285,6 +285,7 @@ struct StageArgs {
     double c[5];       // AB: h*beta_i; RK: c[0] = stage coefficient for aux, c[1] for acc
     int order;
     long long bstride;  // P*Nk
+    long long mstride;  // batch stride of H0 and xi: 0 (one model) or P*Nk (a model per solve)
     int Nk, nb, TK;
 };
 
@@ -339,10 +340,11 @@ __device__ __forceinline__ void load_stage_inputs(const StageArgs& a, const Stag
             el[u] = (long long)p * Nk + k0 + kk;
             if (ok[u]) {
                 r[u] = __ldg(&a.rho[boff + el[u]]);
-                if (!FH) h[u] = __ldg(&a.H0[el[u]]);
-                if (e0) x0[u] = __ldg(&a.xi[0][el[u]]);
-                if (e1) x1[u] = __ldg(&a.xi[1][el[u]]);
-                if (e2) x2[u] = __ldg(&a.xi[2][el[u]]);
+                const long long em = el[u] + (long long)b * a.mstride;
+                if (!FH) h[u] = __ldg(&a.H0[em]);
+                if (e0) x0[u] = __ldg(&a.xi[0][em]);
+                if (e1) x1[u] = __ldg(&a.xi[1][em]);
+                if (e2) x2[u] = __ldg(&a.xi[2][em]);
                 if (COUL) he[u] = __ldg(&a.Hee[boff + el[u]]);
             }
         }

@@ -35,7 +35,7 @@ EXPORTS = [
     "edus_get_stream", "edus_set_profiling", "edus_get_profile", "edus_rhs_noalloc",
     "edus_set_anchor_interval", "edus_state_rspace", "edus_set_fock_override",
     "edus_mlp_create", "edus_mlp_destroy", "edus_mlp_last_error", "edus_mlp_param_count", "edus_mlp_set_params",
-    "edus_mlp_get_params", "edus_mlp_forward", "edus_mlp_gradients", "edus_mlp_train_step",
+    "edus_mlp_get_params", "edus_mlp_forward", "edus_mlp_gradients", "edus_mlp_train_step",    "edus_upload_model_solve", "edus_sweep_step", "edus_autotune",
 ]
 
 
@@ -109,6 +109,9 @@ def load_library(path: str | None = None):
     L.edus_get_profile.argtypes = [h, ctypes.c_int, dp, P(ctypes.c_ulonglong)]
     vp = ctypes.c_void_p
     L.edus_set_anchor_interval.argtypes = [h, ctypes.c_int]
+    L.edus_upload_model_solve.argtypes = [h, ctypes.c_int, dp, dp]
+    L.edus_sweep_step.argtypes = [P(h), ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.edus_autotune.argtypes = [h, P(ctypes.c_int), P(ctypes.c_int)]
     ip = P(ctypes.c_int)
     L.edus_state_rspace.argtypes = [h, ctypes.c_int, ctypes.c_int, ip, dp]
     L.edus_set_fock_override.argtypes = [h, ctypes.c_int, ip, dp]
@@ -273,6 +276,19 @@ class Solver:
     def synchronize(self):
         self._check(self._L.edus_synchronize(self._h))
 
+    def upload_model_solve(self, b, H0k, xik):
+        """A model of its own for solve b (FP64 form without HSEX)."""
+        H = _c128(H0k, self.shape)
+        X = _c128(xik, (3,) + self.shape)
+        self._check(self._L.edus_upload_model_solve(self._h, int(b), _dp(H), _dp(X)))
+
+    def autotune(self):
+        """Time the launch variants on this handle's data and keep the fastest;
+        returns (plane-kernel threads, tensor-core commutator)."""
+        t, c = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(self._L.edus_autotune(self._h, ctypes.byref(t), ctypes.byref(c)))
+        return t.value, bool(c.value)
+
     def set_anchor_interval(self, steps):
         """Split-precision form: steps between moves of the anchor rho_ref."""
         self._check(self._L.edus_set_anchor_interval(self._h, int(steps)))
@@ -310,3 +326,18 @@ class Solver:
         v = ctypes.c_ulonglong()
         self._check(self._L.edus_kernel_launches(self._h, ctypes.byref(v)))
         return v.value
+
+
+def sweep_step(solvers, steps, graph=True):
+    """Advance several Solvers (one device, FP64 form) by `steps` steps
+    together (edus_sweep_step): each on its own stream, chunks of RK4 steps
+    captured into one CUDA graph when `graph`."""
+    if not solvers:
+        return
+    L = solvers[0]._L
+    arr = (ctypes.c_void_p * len(solvers))(*[s._h.value if hasattr(s._h, "value") else s._h for s in solvers])
+    rc = L.edus_sweep_step(ctypes.cast(arr, ctypes.POINTER(ctypes.c_void_p)), len(solvers), int(steps),
+                           1 if graph else 0)
+    if rc:
+        msgs = "; ".join(L.edus_last_error(s._h).decode() for s in solvers if L.edus_last_error(s._h))
+        raise EdusError(rc, msgs)

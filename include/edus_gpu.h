@@ -143,6 +143,13 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k,
                       const double* lattice, const double* W_R, const double* rho0_R,
                       const double* hartree);
 
+/* A model of its own for solve b (batches of solves whose models differ, such
+ * as sweeps over seeded models of one grid and band count): H0_k and xi_k as in
+ * edus_upload_model; the lattice stays the handle's.  Solves without a call
+ * keep the model of edus_upload_model, which must come first.  FP64 form
+ * without HSEX.  No reference counterpart. */
+int edus_upload_model_solve(edus_handle* h, int b, const double* H0_k, const double* xi_k);
+
 /* Lasers of solve `b` (0 <= b < batch).  Replaces SetOfLaser
  * (src/Laser/Laser.hpp:128-170).  n may be 0 (no field). */
 int edus_set_lasers(edus_handle* h, int b, int n, const edus_laser* lasers);
@@ -164,6 +171,20 @@ int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k);
 /* Advance every solve by n steps (DESolver::Propagate(n), DESolver.hpp:238-242).
  * Asynchronous: returns once the work is queued. */
 int edus_step(edus_handle* h, int n);
+
+/* Advance n handles (one device, FP64 form) by `steps` steps together: every
+ * handle's kernels run on its own stream, forked from and joined into one
+ * sweep stream, so solves of different grids and band counts share the GPU.
+ * With use_graph != 0 and RK4 handles, each chunk of 32 steps of all handles
+ * is captured once into one CUDA graph and replayed (the field tables are
+ * refreshed between replays).  Synchronous.  No reference counterpart. */
+int edus_sweep_step(edus_handle* const* hs, int n, int steps, int use_graph);
+
+/* Time the launch variants on the handle's own data and keep the fastest:
+ * the plane kernel's thread count, and (outside the TMA path) the CUDA-core
+ * against the tensor-core commutator.  Either output may be NULL.  Leaves the
+ * state unchanged.  No reference counterpart. */
+int edus_autotune(edus_handle* h, int* plane_threads, int* comm_tensor);
 
 /* rho(R) of solve b at nsel lattice vectors: out[s][n][m] = rho_nm(R_s) with
  * rho(R) = FFT_{-1}(rho_k) / Nk (Operator::go_to_R, Operator.hpp:566-586) and
