@@ -421,9 +421,23 @@ int launch_comm(edus_handle* h, int mode, const StageArgs& a, int nbatch, bool f
     return fail(h, EDUS_ERR_ARG, "bad stage mode");
 }
 
+// The dynamic shared-memory limit is a process-wide attribute of each kernel:
+// every handle sets it to the device's opt-in maximum, so that a handle
+// created later (whatever its sizes) never lowers it below what an earlier
+// handle launches with.  `bytes` is what this handle needs.
+int device_smem_optin(int device) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    return v;
+}
+
 template <typename K>
 int set_smem(edus_handle* h, K kernel, int bytes) {
-    CU(h, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    const int lim = device_smem_optin(h->d.device);
+    if (bytes > lim)
+        return fail(h, EDUS_ERR_UNSUPPORTED,
+                    "needs " + std::to_string(bytes) + " B of shared memory per CTA (device: " + std::to_string(lim) + ")");
+    CU(h, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
     return EDUS_OK;
 }
 
@@ -527,8 +541,7 @@ int launch_pcomm(edus_handle* h, int mode, const PackedArgs& a, int nbatch) {
 
 template <typename K>
 int set_smem_any(edus_handle* h, K kernel, size_t bytes) {
-    CU(h, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    return EDUS_OK;
+    return set_smem(h, kernel, (int)bytes);
 }
 
 template <int MODE, bool COUL>
@@ -1544,8 +1557,19 @@ int edus_sweep_step(edus_handle* const* hs, int n, int steps, int use_graph) {
             cleanup();
             return fail(h0, EDUS_ERR_CUDA, "sweep event creation failed");
         }
+    {
+        const cudaError_t pend = cudaGetLastError();
+        if (pend != cudaSuccess) {
+            cleanup();
+            return fail(h0, EDUS_ERR_CUDA, std::string("sweep set-up: ") + cudaGetErrorString(pend));
+        }
+    }
     // every handle's launches of `cnt` steps, forked from and joined into s0
     auto launch_all = [&](int cnt) -> int {
+        {
+            const cudaError_t pend = cudaGetLastError();
+            if (pend != cudaSuccess) return fail(h0, EDUS_ERR_CUDA, std::string("sweep, before launches: ") + cudaGetErrorString(pend));
+        }
         if (cudaEventRecord(fork, s0) != cudaSuccess) return fail(h0, EDUS_ERR_CUDA, "cudaEventRecord failed");
         for (int i = 0; i < n; ++i) {
             edus_handle* h = hs[i];
