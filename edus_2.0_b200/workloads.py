@@ -292,3 +292,34 @@ def hbn_golden_input(tb_seed: str) -> dict:
 def save_input(d: dict, path: str):
     with open(path, "w") as f:
         json.dump(d, f, indent=2)
+
+
+# ---------------------------------------------------------------------------
+# Batched laser sweep: solves of uneven band count and k grid, each a seeded
+# random tight-binding model (IPA, RK4) under its own Gaussian pulse.
+SWEEP_BANDS = (2, 4, 8, 14, 22)
+SWEEP_SIDES = (24, 36, 48, 72, 96)
+
+
+def sweep_specs(n: int = 256, seed: int = 2024):
+    """n solves: band count and square grid side drawn from SWEEP_BANDS and
+    SWEEP_SIDES, photon energy uniform in [1, 3] eV, peak field log-uniform in
+    [1e-4, 2e-2] a.u., a model seed each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        out.append(dict(nb=int(rng.choice(SWEEP_BANDS)), N=int(rng.choice(SWEEP_SIDES)),
+                        model_seed=int(rng.integers(1 << 30)), photon_eV=float(rng.uniform(1.0, 3.0)),
+                        E0_au=float(10.0 ** rng.uniform(-4.0, math.log10(2e-2)))))
+    return out
+
+
+def sweep_input(spec: dict, outdir: str, dt_fs: float = 0.005, nsteps: int = 1000):
+    """input.json dict of one sweep solve (its model file written in outdir)."""
+    os.makedirs(outdir, exist_ok=True)
+    nb, N = spec["nb"], spec["N"]
+    uc, Rs, H, r = random_model(nb, spec["model_seed"])
+    seed = os.path.join(outdir, f"sweep_{nb}_{spec['model_seed']}")
+    write_tb(seed + "_tb.dat", uc, Rs, H, r, f"random {nb}-band model, seed {spec['model_seed']}")
+    las = [gaussian_laser(spec["photon_eV"], 2.0, spec["E0_au"], 2.5, pol=(1.0, 0.3, 0.0))]
+    return _input(seed, (N, N, 1), max(1, nb // 2), dt_fs, nsteps, "RK", las)
