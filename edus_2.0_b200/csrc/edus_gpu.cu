@@ -52,6 +52,10 @@ struct edus_handle {
     int* hpos = nullptr;
     double2* hval = nullptr;
     int nS = 0;
+    // observables: eigenvectors U_k and velocity operator v_d(k), [P][Nk] each
+    double2* obsU = nullptr;
+    double2* obsV[3] = {nullptr, nullptr, nullptr};
+    double* obsacc = nullptr;
     // a model (H0, xi) per solve (edus_upload_model_solve): [B][P][Nk] each
     bool per_solve = false;
     double2* H0b = nullptr;
@@ -669,6 +673,56 @@ int anchor_split(edus_handle* h) {
     return EDUS_OK;
 }
 
+// One CTA per k point: contributions of that k to the Bloch populations
+// Re (U^dagger rho U)_nn, the Wannier populations Re rho_nn and tr(v_d rho),
+// accumulated in acc[0..nb) (Bloch), acc[nb..2nb) (Wannier), acc[2nb..2nb+6)
+// (re, im of d = 0, 1, 2).  Shared memory: rho_k and U_k, [n][m].
+__global__ void observables_kernel(const double2* __restrict__ rho, const double2* __restrict__ U,
+                                   const double2* __restrict__ v0, const double2* __restrict__ v1,
+                                   const double2* __restrict__ v2, int Nk, int nb, double* __restrict__ acc) {
+    extern __shared__ double2 so[];
+    const int k = blockIdx.x, P = nb * nb;
+    double2* R = so;
+    double2* Us = so + P;
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        R[p] = rho[(long long)p * Nk + k];
+        Us[p] = U ? U[(long long)p * Nk + k] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < nb; n += blockDim.x) {
+        if (U) {
+            double bl = 0.0;
+            for (int i = 0; i < nb; ++i) {
+                double2 t = make_double2(0.0, 0.0);
+                for (int j = 0; j < nb; ++j) t = cadd(t, cmul(R[i * nb + j], Us[j * nb + n]));
+                const double2 u = Us[i * nb + n];
+                bl += u.x * t.x + u.y * t.y;  // Re(conj(u) t)
+            }
+            atomicAdd(&acc[n], bl);
+        }
+        atomicAdd(&acc[nb + n], R[n * nb + n].x);
+    }
+    if (!v0) return;
+    const double2* vs[3] = {v0, v1, v2};
+    double part[6] = {0, 0, 0, 0, 0, 0};
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        const int n = p / nb, l = p - (p / nb) * nb;
+        const double2 r = R[l * nb + n];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double2 c = cmul(vs[d][(long long)p * Nk + k], r);
+            part[2 * d] += c.x;
+            part[2 * d + 1] += c.y;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        double v = part[q];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&acc[2 * nb + q], v);
+    }
+}
+
 // plane position (digit-reversed order) of the natural R index (j0 N1 + j1) N2 + j2
 int position_of(const edus_handle* h, int iR) {
     const int j2 = iR % h->N[2], j1 = (iR / h->N[2]) % h->N[1], j0 = iR / (h->N[1] * h->N[2]);
@@ -887,6 +941,7 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     if ((rc = set_smem(h, plane_rhs_kernel<true, kRadix89, 768>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_rhs_kernel<false, kRadix89, 768>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_to_R_kernel<kRadixAll, 256>, h->Nk * (int)sizeof(double2)))) return bail(rc);
+    if ((rc = set_smem(h, observables_kernel, 2 * h->P * (int)sizeof(double2)))) return bail(rc);
     // the attribute covers both commutator variants, which the autotuner may swap
     const int smem_cmax = (int)std::max(comm_geometry(h->nb).smem, mma_geometry(h->nb).smem);
 #define SETC(M)                                                                                   \
@@ -1236,6 +1291,69 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, co
         h->ref_fixed = false;
     }
     h->model_ready = true;
+    return EDUS_OK;
+}
+
+int edus_upload_observables(edus_handle* h, const double* U_k, const double* vel_k) {
+    if (!h || (!U_k && !vel_k)) return EDUS_ERR_ARG;
+    CU(h, cudaSetDevice(h->d.device));
+    const size_t Sb = h->S * sizeof(double2);
+    int rc;
+    dim3 tb(32, 8), tg((h->Nk + 31) / 32, (h->P + 31) / 32);
+    auto up = [&](const double* src, double2** dst) -> int {
+        int r;
+        if (!*dst && (r = dalloc(h, (void**)dst, Sb))) return r;
+        CU(h, cudaMemcpyAsync(h->stage, src, Sb, cudaMemcpyHostToDevice, h->stream));
+        transpose_kp_to_pk<<<tg, tb, 0, h->stream>>>(h->stage, *dst, h->Nk, h->P);
+        h->launches++;
+        CU(h, cudaGetLastError());
+        CU(h, cudaStreamSynchronize(h->stream));  // h->stage is reused by the next upload
+        return EDUS_OK;
+    };
+    if (U_k && (rc = up(U_k, &h->obsU))) return rc;
+    if (vel_k)
+        for (int d = 0; d < 3; ++d)
+            if ((rc = up(vel_k + 2 * h->S * d, &h->obsV[d]))) return rc;
+    if (!h->obsacc && (rc = dalloc(h, (void**)&h->obsacc, (2 * (size_t)h->nb + 6) * sizeof(double)))) return rc;
+    return EDUS_OK;
+}
+
+int edus_observables(edus_handle* h, int b, int filled, double* pop_bloch, double* pop_wannier, double* vel) {
+    if (!h) return EDUS_ERR_ARG;
+    if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
+    if (pop_bloch && !h->obsU) return fail(h, EDUS_ERR_ARG, "the Bloch populations need edus_upload_observables(U)");
+    if (vel && !h->obsV[0]) return fail(h, EDUS_ERR_ARG, "the velocity needs edus_upload_observables(vel)");
+    int rc;
+    if (!h->obsacc && (rc = dalloc(h, (void**)&h->obsacc, (2 * (size_t)h->nb + 6) * sizeof(double)))) return rc;
+    CU(h, cudaSetDevice(h->d.device));
+    if (h->packed && (rc = unpack_state(h, b))) return rc;
+    const int nacc = 2 * h->nb + 6;
+    CU(h, cudaMemsetAsync(h->obsacc, 0, nacc * sizeof(double), h->stream));
+    observables_kernel<<<h->Nk, 128, 2 * h->P * sizeof(double2), h->stream>>>(
+        h->y + (size_t)b * h->S, pop_bloch ? h->obsU : nullptr, vel ? h->obsV[0] : nullptr, h->obsV[1], h->obsV[2],
+        h->Nk, h->nb, h->obsacc);
+    h->launches++;
+    CU(h, cudaGetLastError());
+    std::vector<double> a(nacc);
+    CU(h, cudaMemcpyAsync(a.data(), h->obsacc, nacc * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    const double inv = 1.0 / h->Nk;
+    for (int n = 0; n < h->nb; ++n) {
+        // Print_Population (Simulation.cpp:439-470): holes of the filled bands in the Bloch gauge
+        if (pop_bloch) pop_bloch[n] = n < filled ? 1.0 - a[n] * inv : a[n] * inv;
+        if (pop_wannier) pop_wannier[n] = a[h->nb + n] * inv;
+    }
+    if (vel)
+        for (int q = 0; q < 6; ++q) vel[q] = a[2 * h->nb + q] * inv;
+    return check_status(h);
+}
+
+int edus_efield(edus_handle* h, int b, double t, double* E) {
+    if (!h || !E) return EDUS_ERR_ARG;
+    if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
+    StageField f;
+    field_at(h->lasers[b], h->A, t, f);
+    for (int d = 0; d < 3; ++d) E[d] = f.E[d];
     return EDUS_OK;
 }
 

@@ -36,6 +36,7 @@ EXPORTS = [
     "edus_set_anchor_interval", "edus_state_rspace", "edus_set_fock_override",
     "edus_mlp_create", "edus_mlp_destroy", "edus_mlp_last_error", "edus_mlp_param_count", "edus_mlp_set_params",
     "edus_mlp_get_params", "edus_mlp_forward", "edus_mlp_gradients", "edus_mlp_train_step",    "edus_upload_model_solve", "edus_sweep_step", "edus_autotune",
+    "edus_upload_observables", "edus_observables", "edus_efield",
 ]
 
 
@@ -110,6 +111,9 @@ def load_library(path: str | None = None):
     vp = ctypes.c_void_p
     L.edus_set_anchor_interval.argtypes = [h, ctypes.c_int]
     L.edus_upload_model_solve.argtypes = [h, ctypes.c_int, dp, dp]
+    L.edus_upload_observables.argtypes = [h, dp, dp]
+    L.edus_observables.argtypes = [h, ctypes.c_int, ctypes.c_int, dp, dp, dp]
+    L.edus_efield.argtypes = [h, ctypes.c_int, ctypes.c_double, dp]
     L.edus_sweep_step.argtypes = [P(h), ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.edus_autotune.argtypes = [h, P(ctypes.c_int), P(ctypes.c_int)]
     ip = P(ctypes.c_int)
@@ -275,6 +279,27 @@ class Solver:
 
     def synchronize(self):
         self._check(self._L.edus_synchronize(self._h))
+
+    def upload_observables(self, U=None, vel=None):
+        """Eigenvectors U [Nk][nb][nb] and/or velocity operator [3][Nk][nb][nb]."""
+        Uc = _c128(U, self.shape) if U is not None else None
+        Vc = _c128(vel, (3,) + self.shape) if vel is not None else None
+        self._check(self._L.edus_upload_observables(self._h, _dp(Uc), _dp(Vc)))
+        self._has_U = getattr(self, "_has_U", False) or U is not None
+        self._has_vel = getattr(self, "_has_vel", False) or vel is not None
+
+    def observables(self, b=0, filled=0):
+        """(Bloch populations, Wannier populations, velocity as 3 complex)."""
+        pb = np.empty(self.nb) if getattr(self, "_has_U", False) else None
+        pw = np.empty(self.nb)
+        v = np.empty(6) if getattr(self, "_has_vel", False) else None
+        self._check(self._L.edus_observables(self._h, int(b), int(filled), _dp(pb), _dp(pw), _dp(v)))
+        return pb, pw, (v[0::2] + 1j * v[1::2]) if v is not None else None
+
+    def efield(self, t, b=0):
+        E = np.empty(3)
+        self._check(self._L.edus_efield(self._h, int(b), float(t), _dp(E)))
+        return E
 
     def upload_model_solve(self, b, H0k, xik):
         """A model of its own for solve b (FP64 form without HSEX)."""

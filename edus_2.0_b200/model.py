@@ -166,6 +166,13 @@ def fft_k_to_R(xk, grid):
     return (np.fft.fftn(a, axes=(0, 1, 2)) / Nk).reshape(xk.shape)
 
 
+def fft_R_to_k(xR, grid):
+    """Operator::go_to_k: FFT sign +1 over the R grid, unnormalised."""
+    Nk = xR.shape[0]
+    a = xR.reshape(*grid, -1)
+    return (np.fft.ifftn(a, axes=(0, 1, 2)) * Nk).reshape(xR.shape)
+
+
 @dataclass
 class Config:
     tb_path: str
@@ -181,6 +188,8 @@ class Config:
     r0: tuple
     lasers: list
     coulomb_fix_centres: bool = False
+    printresolution: int = 1
+    printresolution_pulse: int = 1  # 0 in the input means printresolution
 
     @property
     def nsteps(self):
@@ -229,7 +238,8 @@ def parse_input(src, base_dir=None) -> Config:
     return Config(tb + "_tb.dat", tuple(int(x) for x in d["grid"]), int(d["filledbands"]), dt, ti, tf,
                   edus.SOLVER_AB if d["solver"] == "AB" else edus.SOLVER_RK, int(d["order"]),
                   bool(d["coulomb"]), float(d["epsilon"]), r0, lasers,
-                  bool(user.get("coulomb_fix_centres", False)))
+                  bool(user.get("coulomb_fix_centres", False)), int(d["printresolution"]),
+                  int(d["printresolution_pulse"]) or int(d["printresolution"]))
 
 
 class Model:
@@ -269,6 +279,30 @@ class Model:
         self.W = self.DM0R = self.hartree = None
         if cfg.coulomb:
             self._coulomb(Rs, r)
+
+    def velocity(self):
+        """Velocity operator v_d(k), [3][Nk][nb][nb] (Simulation.cpp:523-576):
+        -i [r_d(k), H0(k)], plus i R_d H0(R) added in R, over the cell area
+        (2-D) or volume (3-D); zero for 1-D grids, which the reference leaves
+        unset."""
+        N = self.grid
+        dims = sum(1 for n in N if n > 1)
+        v = np.zeros((3,) + self.H0k.shape, dtype=np.complex128)
+        if dims < 2:
+            return v
+        A = self.A
+        if dims == 3:
+            det = abs(np.linalg.det(A))
+        else:
+            if N[2] > 1:
+                raise ValueError("perpendicular != 2 -> implement me!")
+            det = abs(A[0, 0] * A[1, 1] - A[1, 0] * A[0, 1])
+        H0R = fft_k_to_R(self.H0k, N)
+        for d in range(3):
+            c = -1j * (self.xik[d] @ self.H0k - self.H0k @ self.xik[d])
+            cR = fft_k_to_R(c, N) + 1j * self.Rcart[:, d][:, None, None] * H0R
+            v[d] = fft_R_to_k(cR, N) / det
+        return v
 
     def _coulomb(self, Rs, r):
         cfg = self.cfg

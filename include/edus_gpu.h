@@ -226,6 +226,23 @@ int edus_set_anchor_interval(edus_handle* h, int steps);
 /* Wait for queued work; reports device-side errors. */
 int edus_synchronize(edus_handle* h);
 
+/* Observables of Simulation::do_onestep (Simulation.cpp:420-429).  Upload once
+ * the eigenvectors U_k [Nk][nb][nb] (columns, SettingUp_EigenSystem) and/or the
+ * velocity operator vel_k [3][Nk][nb][nb] (Simulation.cpp:523-576); either may
+ * be NULL. */
+int edus_upload_observables(edus_handle* h, const double* U_k, const double* vel_k);
+
+/* Observables of solve b's current state (synchronous; any output may be NULL):
+ *   pop_bloch[nb]   (1/Nk) sum_k Re (U^dagger rho U)_nn, as 1 - P_n for the
+ *                   `filled` lowest bands (Print_Population, bloch)
+ *   pop_wannier[nb] (1/Nk) sum_k Re rho_nn (Print_Population, wannier)
+ *   vel[6]          re, im of (1/Nk) sum_k tr(v_d rho), d = x, y, z (Print_Velocity) */
+int edus_observables(edus_handle* h, int b, int filled, double* pop_bloch, double* pop_wannier, double* vel);
+
+/* E(t) of solve b's lasers, the same field the kernels use (SetOfLaser::operator(),
+ * Laser.hpp:143-150). */
+int edus_efield(edus_handle* h, int b, double t, double* E);
+
 /* Observables of solve b for the current state, as Simulation::do_onestep
  * prints them (Simulation.cpp:439-470, 583-622):
  *   pop_wannier[nb] = (1/Nk) sum_k Re rho_nn(k).

@@ -1,0 +1,70 @@
+"""The command-line propagation and the GPU observables.
+
+* cli.run on the reference's hBN integration input (ci-test/inputs/hBN.json.in)
+  writes Population.txt, Velocity.txt, Laser.txt and Time.txt that match the
+  reference's outputs at ci-test/compare.py's 1e-10 (Time.txt is printed with
+  6 significant digits);
+* edus_observables equals the populations and velocity computed on the host
+  from the state, the eigenvectors and the velocity operator.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from test_gpu_parity import model_input
+
+pytestmark = pytest.mark.gpu
+
+
+def test_cli_reproduces_hbn_goldens(pkg, hbn_golden_model, tmp_path):
+    inp = pkg.workloads.hbn_golden_input(hbn_golden_model)
+    path = os.path.join(str(tmp_path), "hBN.json")
+    with open(path, "w") as f:
+        json.dump(inp, f)
+    out = os.path.join(str(tmp_path), "Output")
+    from edus_b200 import cli
+
+    n = cli.run(path, out)
+    assert n == 102
+    for name, tol in (("Population", 1e-10), ("Velocity", 1e-10), ("Laser", 1e-16)):
+        got = np.loadtxt(os.path.join(out, name + ".txt"))
+        ref = np.loadtxt(os.path.join(GOLDEN, "hBN", name + ".txt"))
+        assert got.shape == ref.shape, name
+        assert np.abs(got - ref).max() < tol, name
+    t = np.loadtxt(os.path.join(out, "Time.txt"))
+    assert np.allclose(t, np.loadtxt(os.path.join(GOLDEN, "hBN", "Time.txt")), rtol=1e-5, atol=1e-12)
+    # the vector potential is minus the integral of the field: against a dense
+    # trapezoid integration of the library's own E(t)
+    A = np.loadtxt(os.path.join(out, "Laser_A.txt"))
+    s = pkg.model.Model(pkg.model.parse_input(path)).solver()
+    cfg = pkg.model.parse_input(path)
+    t_print = np.arange(len(A)) * cfg.dt
+    fine = np.linspace(0.0, t_print[-1], 64 * (len(A) - 1) + 1)
+    Ef = np.array([s.efield(t) for t in fine])
+    cum = np.concatenate([[np.zeros(3)], np.cumsum(0.5 * (Ef[1:] + Ef[:-1]) * np.diff(fine)[:, None], axis=0)])
+    ref_A = -cum[::64]
+    assert np.abs(A - ref_A).max() < 1e-6 * max(np.abs(ref_A).max(), 1e-30)
+
+
+def test_observables_match_host(pkg, tmp_path):
+    inp = model_input(pkg, tmp_path, "obs", (8, 6, 1), nb=4, coulomb=True, dt=0.01, envelope="gauss")
+    cfg = pkg.model.parse_input(inp)
+    m = pkg.model.Model(cfg)
+    s = m.solver()
+    vel = m.velocity()
+    s.upload_observables(U=m.U, vel=vel)
+    s.step(20)
+    rho = s.get_state()
+    pb, pw, v = s.observables(0, cfg.filledbands)
+    rb = np.einsum("kji,kjl,klm->kim", m.U.conj(), rho, m.U)
+    ref_b = np.real(np.einsum("knn->n", rb)) / m.Nk
+    ref_b[: cfg.filledbands] = 1.0 - ref_b[: cfg.filledbands]
+    ref_w = np.real(np.einsum("knn->n", rho)) / m.Nk
+    ref_v = np.array([np.einsum("knl,kln->", vel[d], rho) / m.Nk for d in range(3)])
+    assert np.abs(pb - ref_b).max() < 1e-13
+    assert np.abs(pw - ref_w).max() < 1e-13
+    assert np.abs(v - ref_v).max() < 1e-13 * max(1.0, np.abs(ref_v).max())
+    assert np.abs(ref_v).max() > 1e-8  # a real signal
