@@ -52,6 +52,10 @@ struct edus_handle {
     int* hpos = nullptr;
     double2* hval = nullptr;
     int nS = 0;
+    // gradient_space "k": finite-difference stencil (edus_set_kgradient)
+    int kg_n = 0, kg_cap = 0;
+    int* kg_shift = nullptr;     // [n][3]
+    double* kg_coef = nullptr;   // [n][4]: b_x, b_y, b_z, w
     // observables: eigenvectors U_k and velocity operator v_d(k), [P][Nk] each
     double2* obsU = nullptr;
     double2* obsV[3] = {nullptr, nullptr, nullptr};
@@ -236,6 +240,48 @@ void prof_resolve(edus_handle* h) {
     h->prof_pending.clear();
 }
 
+// gradient_space "k" (kGradient_definitions.hpp:18-30): G[b][p][k] =
+// sum_i w_i (b_i.E) rho[b][p][k + b_i], k + b_i folded into the grid.  The
+// coefficients of the CTA's solve are formed once in shared memory.
+__global__ void kgradient_kernel(const double2* __restrict__ rho, long long in_bstride, double2* __restrict__ G,
+                                 long long out_bstride, const int* __restrict__ shift, const double* __restrict__ coef,
+                                 int n,
+                                 const StageField* __restrict__ field, int N0, int N1, int N2, int P) {
+    extern __shared__ double kc[];  // [n] coefficients
+    int* ks = reinterpret_cast<int*>(kc + n);  // [n][3] shifts
+    const int b = blockIdx.y;
+    const StageField F = field[b];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        kc[i] = coef[4 * i + 3] * (coef[4 * i] * F.E[0] + coef[4 * i + 1] * F.E[1] + coef[4 * i + 2] * F.E[2]);
+        ks[3 * i] = shift[3 * i];
+        ks[3 * i + 1] = shift[3 * i + 1];
+        ks[3 * i + 2] = shift[3 * i + 2];
+    }
+    __syncthreads();
+    const int Nk = N0 * N1 * N2;
+    const long long total = (long long)P * Nk;
+    const double2* src = rho + (long long)b * in_bstride;
+    double2* dst = G + (long long)b * out_bstride;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int p = (int)(e / Nk), k = (int)(e - (long long)p * Nk);
+        const int j2 = k % N2, j1 = (k / N2) % N1, j0 = k / (N1 * N2);
+        const double2* plane = src + (long long)p * Nk;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int i = 0; i < n; ++i) {
+            const double c = kc[i];
+            if (c == 0.0) continue;
+            int a0 = j0 + ks[3 * i], a1 = j1 + ks[3 * i + 1], a2 = j2 + ks[3 * i + 2];
+            a0 -= a0 >= N0 ? N0 : 0;
+            a1 -= a1 >= N1 ? N1 : 0;
+            a2 -= a2 >= N2 ? N2 : 0;
+            const double2 v = __ldg(&plane[(a0 * N1 + a1) * N2 + a2]);
+            acc.x += c * v.x;
+            acc.y += c * v.y;
+        }
+        dst[e] = acc;
+    }
+}
+
 template <bool COUL, int MASK, int MAXT>
 void launch_plane_variant(edus_handle* h, dim3 grid, const double2* in, long long in_bstride, double2* G,
                           double2* Hee, long long out_bstride, const StageField* field, int nS) {
@@ -295,6 +341,24 @@ int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double
     dim3 grid(h->P, nbatch);
     cudaEvent_t e0;
     prof_begin(h, &e0);
+    const bool c = h->d.coulomb != 0;
+    const int nS = (fuse && c) ? h->nS : 0;
+    // gradient_space "k": the stencil kernel writes G; without HSEX it is the
+    // only launch, with HSEX it follows the plane kernel (whose g is zero)
+    const bool kmode = h->kg_n > 0 && !h->split && !h->packed;
+    auto launch_kgrad = [&]() {
+        const long long total = (long long)h->P * h->Nk;
+        dim3 kg((unsigned)std::min<long long>((total + 255) / 256, 148LL * 16), nbatch);
+        kgradient_kernel<<<kg, 256, h->kg_n * (sizeof(double) + 3 * sizeof(int)), h->stream>>>(
+            in, in_bstride, G, out_bstride, h->kg_shift, h->kg_coef, h->kg_n, field, h->N[0], h->N[1], h->N[2], h->P);
+        h->launches++;
+    };
+    if (kmode && !c) {
+        launch_kgrad();
+        CU(h, cudaGetLastError());
+        prof_end(h, 0, e0);
+        return EDUS_OK;
+    }
     if (h->split && fuse) {
         launch_split(h, in, G, Hee, field, nbatch);
         h->launches++;
@@ -302,8 +366,6 @@ int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double
         prof_end(h, 0, e0);
         return EDUS_OK;
     }
-    const bool c = h->d.coulomb != 0;
-    const int nS = (fuse && c) ? h->nS : 0;
     if (h->plane_cfg.persist) {
         const int np = h->P * nbatch;
         if (h->plane_cfg.variant == 1) {
@@ -321,6 +383,7 @@ int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double
         else launch_plane_variant<false, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, nS);
     }
     h->launches++;
+    if (kmode) launch_kgrad();
     CU(h, cudaGetLastError());
     prof_end(h, 0, e0);
     return EDUS_OK;
@@ -942,6 +1005,7 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     if ((rc = set_smem(h, plane_rhs_kernel<false, kRadix89, 768>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_to_R_kernel<kRadixAll, 256>, h->Nk * (int)sizeof(double2)))) return bail(rc);
     if ((rc = set_smem(h, observables_kernel, 2 * h->P * (int)sizeof(double2)))) return bail(rc);
+    if ((rc = set_smem(h, kgradient_kernel, 4096 * (int)(sizeof(double) + 3 * sizeof(int))))) return bail(rc);
     // the attribute covers both commutator variants, which the autotuner may swap
     const int smem_cmax = (int)std::max(comm_geometry(h->nb).smem, mma_geometry(h->nb).smem);
 #define SETC(M)                                                                                   \
@@ -1294,6 +1358,41 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, co
     return EDUS_OK;
 }
 
+int edus_set_kgradient(edus_handle* h, int n, const int* shift, const double* b, const double* w) {
+    if (!h || n < 0 || (n > 0 && (!shift || !b || !w))) return EDUS_ERR_ARG;
+    if (n == 0) {
+        CU(h, cudaStreamSynchronize(h->stream));
+        h->kg_n = 0;
+        return EDUS_OK;
+    }
+    if (h->packed || h->split)
+        return fail(h, EDUS_ERR_UNSUPPORTED, "gradient_space \"k\" is implemented for the FP64 form");
+    if (n > 4096) return fail(h, EDUS_ERR_ARG, "k-gradient stencil longer than 4096 vectors");
+    std::vector<int> sh(3 * (size_t)n);
+    std::vector<double> cf(4 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        for (int d = 0; d < 3; ++d) {
+            int x = shift[3 * i + d] % h->N[d];
+            if (x < 0) x += h->N[d];
+            sh[3 * i + d] = x;
+            cf[4 * i + d] = b[3 * i + d];
+        }
+        cf[4 * i + 3] = w[i];
+    }
+    CU(h, cudaSetDevice(h->d.device));
+    CU(h, cudaStreamSynchronize(h->stream));
+    int rc;
+    if (n > h->kg_cap) {
+        if ((rc = dalloc(h, (void**)&h->kg_shift, 3 * (size_t)n * sizeof(int)))) return rc;
+        if ((rc = dalloc(h, (void**)&h->kg_coef, 4 * (size_t)n * sizeof(double)))) return rc;
+        h->kg_cap = n;
+    }
+    CU(h, cudaMemcpy(h->kg_shift, sh.data(), sh.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CU(h, cudaMemcpy(h->kg_coef, cf.data(), cf.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->kg_n = n;
+    return EDUS_OK;
+}
+
 int edus_upload_observables(edus_handle* h, const double* U_k, const double* vel_k) {
     if (!h || (!U_k && !vel_k)) return EDUS_ERR_ARG;
     CU(h, cudaSetDevice(h->d.device));
@@ -1481,6 +1580,7 @@ int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k) {
     // previous user of the pinned buffer)
     CU(h, cudaEventSynchronize(h->field_ev[0]));
     field_at(h->lasers[0], h->A, t, h->field_host[0][0]);
+    if (h->kg_n > 0) h->field_host[0][0].g[0] = h->field_host[0][0].g[1] = h->field_host[0][0].g[2] = 0.0;
     CU(h, cudaMemcpyAsync(h->field, h->field_host[0], sizeof(StageField), cudaMemcpyHostToDevice, h->stream));
     CU(h, cudaEventRecord(h->field_ev[0], h->stream));
     dim3 tb(32, 8), tg((h->Nk + 31) / 32, (h->P + 31) / 32);
@@ -1512,7 +1612,11 @@ static void fill_field_table(edus_handle* h, int cnt, StageField* tab) {
     for (int i = 0; i < cnt; ++i) {
         double ts[4] = {t, t + dt / 2., t + dt / 2., t + dt};
         for (int s = 0; s < nst; ++s)
-            for (int b = 0; b < h->B; ++b) field_at(h->lasers[b], h->A, ts[s], tab[((size_t)i * nst + s) * h->B + b]);
+            for (int b = 0; b < h->B; ++b) {
+                StageField& f = tab[((size_t)i * nst + s) * h->B + b];
+                field_at(h->lasers[b], h->A, ts[s], f);
+                if (h->kg_n > 0) f.g[0] = f.g[1] = f.g[2] = 0.0;  // the gradient is the k stencil
+            }
         t += dt;
     }
 }

@@ -36,7 +36,7 @@ EXPORTS = [
     "edus_set_anchor_interval", "edus_state_rspace", "edus_set_fock_override",
     "edus_mlp_create", "edus_mlp_destroy", "edus_mlp_last_error", "edus_mlp_param_count", "edus_mlp_set_params",
     "edus_mlp_get_params", "edus_mlp_forward", "edus_mlp_gradients", "edus_mlp_train_step",    "edus_upload_model_solve", "edus_sweep_step", "edus_autotune",
-    "edus_upload_observables", "edus_observables", "edus_efield",
+    "edus_upload_observables", "edus_observables", "edus_efield", "edus_set_kgradient",
 ]
 
 
@@ -112,6 +112,7 @@ def load_library(path: str | None = None):
     L.edus_set_anchor_interval.argtypes = [h, ctypes.c_int]
     L.edus_upload_model_solve.argtypes = [h, ctypes.c_int, dp, dp]
     L.edus_upload_observables.argtypes = [h, dp, dp]
+    L.edus_set_kgradient.argtypes = [h, ctypes.c_int, P(ctypes.c_int), dp, dp]
     L.edus_observables.argtypes = [h, ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.edus_efield.argtypes = [h, ctypes.c_int, ctypes.c_double, dp]
     L.edus_sweep_step.argtypes = [P(h), ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -279,6 +280,18 @@ class Solver:
 
     def synchronize(self):
         self._check(self._L.edus_synchronize(self._h))
+
+    def set_kgradient(self, shift=None, b=None, w=None):
+        """gradient_space "k": the finite-difference stencil (model.kgradient_stencil);
+        no arguments restores the R-space gradient."""
+        if shift is None:
+            self._check(self._L.edus_set_kgradient(self._h, 0, None, None, None))
+            return
+        sh = np.ascontiguousarray(shift, dtype=np.int32)
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        ww = np.ascontiguousarray(w, dtype=np.float64)
+        self._check(self._L.edus_set_kgradient(self._h, len(ww), sh.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                               _dp(bb), _dp(ww)))
 
     def upload_observables(self, U=None, vel=None):
         """Eigenvectors U [Nk][nb][nb] and/or velocity operator [3][Nk][nb][nb]."""

@@ -190,6 +190,7 @@ class Config:
     coulomb_fix_centres: bool = False
     printresolution: int = 1
     printresolution_pulse: int = 1  # 0 in the input means printresolution
+    gradient_space: str = "R"  # "k": finite-difference gradient over k shells
 
     @property
     def nsteps(self):
@@ -239,7 +240,7 @@ def parse_input(src, base_dir=None) -> Config:
                   edus.SOLVER_AB if d["solver"] == "AB" else edus.SOLVER_RK, int(d["order"]),
                   bool(d["coulomb"]), float(d["epsilon"]), r0, lasers,
                   bool(user.get("coulomb_fix_centres", False)), int(d["printresolution"]),
-                  int(d["printresolution_pulse"]) or int(d["printresolution"]))
+                  int(d["printresolution_pulse"]) or int(d["printresolution"]), str(d["gradient_space"]))
 
 
 class Model:
@@ -279,6 +280,51 @@ class Model:
         self.W = self.DM0R = self.hartree = None
         if cfg.coulomb:
             self._coulomb(Rs, r)
+
+    def kgradient_stencil(self):
+        """Finite-difference k gradient of gradient_space "k" (kGradient.cpp:26-211,
+        Mostofi et al., CPC 178 (2008) 685): (shift [n][3] FFT index of b,
+        b [n][3] Cartesian 1/bohr, w [n]) with E.grad f(k) = sum w (b.E) f(k + b)
+        over the fewest shells of equal |b| whose A w = q has an exact solution."""
+        N = self.grid
+        B = 2.0 * PI * np.linalg.inv(self.A).T  # columns: reciprocal vectors
+        i0, i1, i2 = np.meshgrid(np.arange(N[0]), np.arange(N[1]), np.arange(N[2]), indexing="ij")
+        j = np.stack([i0, i1, i2], -1).reshape(-1, 3)
+        x = j / np.array(N, dtype=np.float64)
+        for d in range(3):  # Gamma-centred crystal coordinates in [-1/2, 1/2)
+            c = x[:, d]
+            c = np.where((c < -0.5) & (np.abs(c + 0.5) > THRESHOLD), c + 1.0, c)
+            c = np.where((c > 0.5) | (np.abs(c - 0.5) < THRESHOLD), c - 1.0, c)
+            x[:, d] = c
+        kc = x @ B.T
+        norm = np.linalg.norm(kc, axis=1)
+        knorms = []
+        for v in norm:
+            if not any(abs(v - kn) < THRESHOLD for kn in knorms):
+                knorms.append(v)
+        knorms.sort()
+        shells = [[] for _ in knorms]
+        for ik, v in enumerate(norm):
+            for sh, kn in enumerate(knorms):
+                if abs(kn - v) < 1e-7:
+                    shells[sh].append(ik)
+                    break
+        if abs(knorms[0]) > THRESHOLD:
+            raise ValueError("k mesh without k = 0")
+        shells = shells[1:]
+        q = np.array([N[0] > 1, N[1] > 1, N[2] > 1, 0, 0, 0], dtype=np.float64)
+        al, be = [0, 1, 2, 0, 0, 1], [0, 1, 2, 1, 2, 2]
+        for ns in range(1, len(shells) + 1):
+            A = np.array([[sum(kc[ik, al[jj]] * kc[ik, be[jj]] for ik in shells[sh]) for sh in range(ns)]
+                          for jj in range(6)])
+            w = np.linalg.pinv(A) @ q
+            if np.linalg.norm(A @ w - q) < THRESHOLD:
+                break
+        else:
+            raise ValueError("k gradient: no set of shells solves A w = q")
+        idx = [ik for sh in range(ns) for ik in shells[sh]]
+        ww = [w[sh] for sh in range(ns) for _ in shells[sh]]
+        return j[idx].astype(np.int32), kc[idx], np.array(ww)
 
     def velocity(self):
         """Velocity operator v_d(k), [3][Nk][nb][nb] (Simulation.cpp:523-576):
@@ -371,6 +417,8 @@ class Model:
             s.upload_model(self.H0k, self.xik, self.A, self.W, self.DM0R, self.hartree)
         else:
             s.upload_model(self.H0k, self.xik, self.A)
+        if cfg.gradient_space == "k":
+            s.set_kgradient(*self.kgradient_stencil())
         for b in range(batch):
             s.set_lasers(cfg.lasers, b)
             s.set_state(self.rho0k, b)

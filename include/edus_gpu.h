@@ -226,6 +226,14 @@ int edus_set_anchor_interval(edus_handle* h, int steps);
 /* Wait for queued work; reports device-side errors. */
 int edus_synchronize(edus_handle* h);
 
+/* gradient_space "k" (kGradient_definitions.hpp:18-30): E.grad_k rho(k) =
+ * sum_i w[i] (b_i.E) rho(k + b_i) over n vectors b_i (Cartesian, 1/bohr,
+ * b[3i..3i+2]) whose grid offsets are shift[3i..3i+2] (FFT indices, folded);
+ * the shells and weights of kGradient.cpp:26-211 are the caller's (one-off
+ * set-up).  Replaces the R-space gradient: without HSEX no plane transform
+ * runs.  n = 0 restores the R-space gradient.  FP64 form. */
+int edus_set_kgradient(edus_handle* h, int n, const int* shift, const double* b, const double* w);
+
 /* Observables of Simulation::do_onestep (Simulation.cpp:420-429).  Upload once
  * the eigenvectors U_k [Nk][nb][nb] (columns, SettingUp_EigenSystem) and/or the
  * velocity operator vel_k [3][Nk][nb][nb] (Simulation.cpp:523-576); either may

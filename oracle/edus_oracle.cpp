@@ -284,6 +284,7 @@ typedef struct {
     // (W_nm(R) + W_mn(-R)) / 2.  This is what the packed-Hermitian GPU forms
     // propagate; it differs from the reference only on the N/2 planes.
     int hermitian_nyquist;
+    int gradient_k;  // 1: gradient_space "k", the finite-difference gradient of kGradient.cpp
     int nlasers;
     oracle_laser lasers[8];
 } oracle_cfg;
@@ -292,6 +293,8 @@ typedef struct {
 
 namespace oracle {
 
+struct Sim;
+void build_kgradient(Sim& s);
 struct Sim {
     int N[3], Nk, nb, P;
     double A[3][3];  // columns = lattice vectors (bohr), src/Model/Model.hpp:41-44
@@ -300,6 +303,10 @@ struct Sim {
     std::vector<double> Rcart;   // [Nk][3] Gamma-centred Cartesian R of FFT index
     std::vector<double> Rcrys;   // [Nk][3]
     std::vector<double> Rgrad;   // [Nk][3] Cartesian R used by the k-gradient
+    // gradient_space "k": stencil k -> k + b over the shells of kGradient.cpp
+    std::vector<std::array<int, 3>> gshift;     // FFT index of b per axis
+    std::vector<std::array<double, 3>> gvec;    // b, Cartesian (1/bohr)
+    std::vector<double> gw;                     // weight of b's shell
     std::vector<double> eval;    // [Nk][nb]
     std::vector<cd> U;           // [Nk][nb][nb]
     std::vector<cd> vel[3];      // velocity operator in k
@@ -438,6 +445,7 @@ Sim* build(const oracle_cfg* cfg) {
         for (int a = 0; a < 3; ++a) s.Rcart[3 * iR + a] = s.A[a][0] * c[0] + s.A[a][1] * c[1] + s.A[a][2] * c[2];
     }
     s.Rgrad = s.Rcart;
+    if (cfg->gradient_k) build_kgradient(s);
     if (cfg->hermitian_nyquist) {
         for (int iR = 0; iR < Nk; ++iR) {
             double c[3];
@@ -613,6 +621,115 @@ Sim* build(const oracle_cfg* cfg) {
     return sim.release();
 }
 
+// Finite-difference k gradient (src/kGradient/kGradient.cpp:26-211, after
+// Mostofi et al., CPC 178 (2008) 685): the Gamma-centred k mesh (crystal
+// coordinates in [-1/2, 1/2), MeshGrid.cpp:458-486; Cartesian k = B k_crys,
+// B = 2 pi A^-T, Model.hpp:46) sorted into shells of equal |b| (k = 0 removed);
+// the fewest shells whose matrix A(j, s) = sum_{b in s} b_alpha b_beta (six
+// (alpha, beta) pairs) solves A w = q exactly by its pseudo-inverse, q = (1
+// per axis with N > 1, 0, 0, 0).  Then E.grad f(k) = sum_s w_s sum_{b in s}
+// (b.E) f(k + b).
+void build_kgradient(Sim& s) {
+    const int Nk = s.Nk;
+    // B = 2 pi (A^-1)^T, columns the reciprocal vectors
+    const double (&A)[3][3] = s.A;
+    const double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                       A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                       A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+    double inv[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            const int i1 = (j + 1) % 3, i2 = (j + 2) % 3, j1 = (i + 1) % 3, j2 = (i + 2) % 3;
+            inv[i][j] = (A[i1][j1] * A[i2][j2] - A[i1][j2] * A[i2][j1]) / det;
+        }
+    double B[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) B[i][j] = 2. * pi * inv[j][i];
+    std::vector<std::array<double, 3>> kc(Nk);
+    std::vector<std::array<int, 3>> kj(Nk);
+    std::vector<double> norm(Nk);
+    for (int ik = 0; ik < Nk; ++ik) {
+        const int j[3] = {ik / (s.N[1] * s.N[2]), (ik / s.N[2]) % s.N[1], ik % s.N[2]};
+        double c[3];
+        for (int d = 0; d < 3; ++d) {
+            double x = (double)j[d] / s.N[d];
+            while (x < -0.5 && std::abs(x + 0.5) > threshold) x += 1.;
+            while (x > 0.5 || std::abs(x - 0.5) < threshold) x -= 1.;
+            c[d] = x;
+            kj[ik][d] = j[d];
+        }
+        for (int a = 0; a < 3; ++a) kc[ik][a] = B[a][0] * c[0] + B[a][1] * c[1] + B[a][2] * c[2];
+        norm[ik] = std::sqrt(kc[ik][0] * kc[ik][0] + kc[ik][1] * kc[ik][1] + kc[ik][2] * kc[ik][2]);
+    }
+    // SortInShells (kGradient.cpp:44-83)
+    std::vector<double> knorms;
+    for (int ik = 0; ik < Nk; ++ik) {
+        bool found = false;
+        for (double kn : knorms) found |= std::abs(kn - norm[ik]) < threshold;
+        if (!found) knorms.push_back(norm[ik]);
+    }
+    std::sort(knorms.begin(), knorms.end());
+    std::vector<std::vector<int>> shells(knorms.size());
+    for (int ik = 0; ik < Nk; ++ik)
+        for (size_t sh = 0; sh < knorms.size(); ++sh)
+            if (std::abs(knorms[sh] - norm[ik]) < 1.e-07) {
+                shells[sh].push_back(ik);
+                break;
+            }
+    if (knorms.empty() || std::abs(knorms[0]) > threshold) throw std::runtime_error("k mesh without k = 0");
+    shells.erase(shells.begin());
+    // Calculate_nshellsAndweights (kGradient.cpp:86-122)
+    const double q[6] = {s.N[0] > 1 ? 1. : 0., s.N[1] > 1 ? 1. : 0., s.N[2] > 1 ? 1. : 0., 0., 0., 0.};
+    const int al[6] = {0, 1, 2, 0, 0, 1}, be[6] = {0, 1, 2, 1, 2, 2};
+    std::vector<double> w;
+    int ns = 0;
+    for (ns = 1; ns <= (int)shells.size(); ++ns) {
+        std::vector<double> Am(6 * ns, 0.);  // A(j, s)
+        for (int j = 0; j < 6; ++j)
+            for (int sh = 0; sh < ns; ++sh)
+                for (int ik : shells[sh]) Am[j * ns + sh] += kc[ik][al[j]] * kc[ik][be[j]];
+        // pseudo-inverse: A^+ = (A^T A)^+ A^T, (A^T A)^+ from its eigen-decomposition
+        std::vector<cd> M((size_t)ns * ns), V((size_t)ns * ns);
+        std::vector<double> lam(ns);
+        for (int a = 0; a < ns; ++a)
+            for (int b = 0; b < ns; ++b) {
+                double x = 0.;
+                for (int j = 0; j < 6; ++j) x += Am[j * ns + a] * Am[j * ns + b];
+                M[(size_t)a * ns + b] = x;
+            }
+        eigh(ns, M.data(), lam.data(), V.data());
+        double lmax = 0.;
+        for (double l : lam) lmax = std::max(lmax, std::abs(l));
+        std::vector<double> Atq(ns, 0.);
+        for (int a = 0; a < ns; ++a)
+            for (int j = 0; j < 6; ++j) Atq[a] += Am[j * ns + a] * q[j];
+        w.assign(ns, 0.);
+        for (int e = 0; e < ns; ++e) {
+            if (std::abs(lam[e]) <= 1e-12 * lmax) continue;
+            double proj = 0.;
+            for (int a = 0; a < ns; ++a) proj += V[(size_t)a * ns + e].real() * Atq[a];
+            for (int a = 0; a < ns; ++a) w[a] += V[(size_t)a * ns + e].real() * proj / lam[e];
+        }
+        double res = 0.;
+        for (int j = 0; j < 6; ++j) {
+            double x = -q[j];
+            for (int sh = 0; sh < ns; ++sh) x += Am[j * ns + sh] * w[sh];
+            res += x * x;
+        }
+        if (std::sqrt(res) < threshold) break;
+    }
+    if (ns > (int)shells.size()) throw std::runtime_error("k gradient: no set of shells solves A w = q");
+    s.gshift.clear();
+    s.gvec.clear();
+    s.gw.clear();
+    for (int sh = 0; sh < ns; ++sh)
+        for (int ik : shells[sh]) {
+            s.gshift.push_back(kj[ik]);
+            s.gvec.push_back(kc[ik]);
+            s.gw.push_back(w[sh]);
+        }
+}
+
 // SourceTerm: src/Simulation/Functional_SourceTerm.hpp:10-56
 void source_term(Sim& s, cd* out_k, double time, const cd* in_k) {
     const int P = s.P, nb = s.nb;
@@ -623,7 +740,7 @@ void source_term(Sim& s, cd* out_k, double time, const cd* in_k) {
     s.efield(time, E);
     // kGradient R branch: out(R) += 1 * i (R.E) in(R)  (kGradient_definitions.hpp:35-40)
 #pragma omp parallel for schedule(static)
-    for (int iR = 0; iR < s.Nk; ++iR) {
+    for (int iR = 0; iR < (s.gw.empty() ? s.Nk : 0); ++iR) {
         const double* Rc = &s.Rgrad[3 * (size_t)iR];
         double dot = Rc[0] * E[0] + Rc[1] * E[1] + Rc[2] * E[2];
         for (int p = 0; p < P; ++p) s.outR[(size_t)iR * P + p] += (1. + 0. * im) * im * dot * s.inR[(size_t)iR * P + p];
@@ -644,6 +761,21 @@ void source_term(Sim& s, cd* out_k, double time, const cd* in_k) {
         for (long i = 0; i < (long)S; ++i) s.HR[i] -= s.W[i] * (s.inR[i] - s.DM0R[i]);
     }
     s.fft.run(s.outR.data(), out_k, +1);                       // :49 Output.go_to_k
+    if (!s.gw.empty()) {
+        // kGradient k branch (kGradient_definitions.hpp:18-30): out(k) += sum w (b.E) in(k + b)
+#pragma omp parallel for schedule(static)
+        for (int ik = 0; ik < s.Nk; ++ik) {
+            const int j[3] = {ik / (s.N[1] * s.N[2]), (ik / s.N[2]) % s.N[1], ik % s.N[2]};
+            for (size_t i = 0; i < s.gw.size(); ++i) {
+                const double c = s.gw[i] * (s.gvec[i][0] * E[0] + s.gvec[i][1] * E[1] + s.gvec[i][2] * E[2]);
+                if (c == 0.) continue;
+                const int jn[3] = {(j[0] + s.gshift[i][0]) % s.N[0], (j[1] + s.gshift[i][1]) % s.N[1],
+                                   (j[2] + s.gshift[i][2]) % s.N[2]};
+                const size_t kn = ((size_t)jn[0] * s.N[1] + jn[1]) * s.N[2] + jn[2];
+                for (int p = 0; p < P; ++p) out_k[(size_t)ik * P + p] += c * in_k[kn * P + p];
+            }
+        }
+    }
     s.fft.run(s.HR.data(), s.Hk.data(), +1);                   // :50 H.go_to_k
     // commutator(Out, -i, H, rho, false) (BlockMatrix_definitions.hpp:203-226)
 #pragma omp parallel for schedule(static)

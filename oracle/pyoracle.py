@@ -194,7 +194,7 @@ class _Cfg(ctypes.Structure):
                 ("solver", ctypes.c_int), ("order", ctypes.c_int), ("coulomb", ctypes.c_int),
                 ("epsilon", ctypes.c_double), ("r0_au", ctypes.c_double * 3),
                 ("nr0", ctypes.c_int), ("coulomb_fix_centres", ctypes.c_int),
-                ("hermitian_nyquist", ctypes.c_int),
+                ("hermitian_nyquist", ctypes.c_int), ("gradient_k", ctypes.c_int),
                 ("nlasers", ctypes.c_int), ("lasers", _Laser * 8)]
 
 
@@ -261,6 +261,7 @@ def make_cfg(cfg: SimConfig) -> _Cfg:
     c.nr0 = len(cfg.r0)
     c.coulomb_fix_centres = int(cfg.coulomb_fix_centres)
     c.hermitian_nyquist = int(cfg.hermitian_nyquist)
+    c.gradient_k = 1 if cfg.gradient_space == "k" else 0
     if len(cfg.lasers) > 8:
         raise ValueError("at most 8 lasers")
     c.nlasers = len(cfg.lasers)

@@ -269,3 +269,47 @@ def test_hbn_generator_matches_reference_model(po, hbn_golden_model):
     for name in ("H0k", "xk", "yk", "zk", "rho"):
         assert np.array_equal(a.get(name), b.get(name)), name
     assert np.array_equal(a.lattice(), b.lattice())
+
+
+def test_k_gradient_converges_to_R_gradient(po, pkg, tmp_path):
+    """gradient_space "k" (the finite-difference shells of kGradient.cpp) on a
+    plane wave rho(k) = exp(i k.R0): it tends to the exact R-space gradient
+    i (R0.E) rho as the grid is refined, with error O((b.R0)^2)."""
+    uc = [[2.1650635094610966, 1.25, 0.0], [2.1650635094610966, -1.25, 0.0], [0, 0, 20.0]]
+    H = np.zeros((1, 1, 1), complex)
+    r = np.zeros((3, 1, 1, 1), complex)
+    seed = os.path.join(str(tmp_path), "flatk")
+    pkg.workloads.write_tb(seed + "_tb.dat", uc, [(0, 0, 0)], H, r)
+    errs = []
+    for N in (12, 24, 48):
+        inp = pkg.workloads._input(seed, (N, N, 1), 0, 0.01, 10, "RK",
+                                   [pkg.workloads.sin2_laser(3.0, 1e12, 4, pol=(0.3, 1.0, 0))])
+        inp["gradient_space"] = "k"
+        cfg = po.load_input(inp)
+        o = po.Oracle(cfg)
+        t = 7.0
+        E = o.efield(t)
+        A = o.lattice()
+        i0, i1 = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
+        phase = np.exp(2j * np.pi * (i0 * 1 + i1 * 0) / N).reshape(-1, 1, 1)
+        out = o.rhs(t, phase)
+        ana = 1j * ((A @ np.array([1.0, 0.0, 0.0])) @ E) * phase
+        errs.append(np.abs(out - ana).max() / np.abs(ana).max())
+    assert errs[0] > errs[1] > errs[2] and errs[2] < 3e-3
+    assert errs[1] / errs[2] > 3.5  # second order
+
+
+def test_k_gradient_stencil_model_equals_property(pkg, tmp_path):
+    """The stencil of model.py satisfies sum_b w b_alpha b_beta = delta (per periodic axis)."""
+    for grid in ((12, 12, 1), (9, 1, 1), (4, 3, 5)):
+        dims = 1 if grid[1] == 1 else (3 if grid[2] > 1 else 2)
+        uc, Rs, H, r = pkg.workloads.random_model(2, 0, dims=dims)
+        seed = os.path.join(str(tmp_path), f"ks{grid[0]}")
+        pkg.workloads.write_tb(seed + "_tb.dat", uc, Rs, H, r)
+        inp = pkg.workloads._input(seed, grid, 1, 0.01, 10, "RK", [])
+        m = pkg.model.Model(pkg.model.parse_input(inp))
+        sh, b, w = m.kgradient_stencil()
+        M = np.einsum("i,ia,ib->ab", w, b, b)
+        want = np.diag([1.0 if n > 1 else 0.0 for n in grid])
+        assert np.abs(M - want).max() < 1e-8
+        assert np.abs(np.einsum("i,ia->a", w, b)).max() < 1e-8  # symmetric shells
