@@ -17,6 +17,7 @@
 #include "packed_kernels.cuh"
 #include "comm_pipe.cuh"
 #include "split_kernels.cuh"
+#include "plane3.cuh"
 #include <cudaTypedefs.h>
 #include <map>
 #include <mutex>
@@ -52,6 +53,12 @@ struct edus_handle {
     int* hpos = nullptr;
     double2* hval = nullptr;
     int nS = 0;
+    // few planes on a 2-D grid: plane transforms over many CTAs (plane3.cuh)
+    bool use3 = false;
+    Plane3Plan p3{};
+    double2* s3a = nullptr;  // rows pass output, [B][P][Nk]
+    double2* s3g = nullptr;  // columns pass: G and H, [B][P][Nk]
+    double2* s3h = nullptr;
     // gradient_space "k": finite-difference stencil (edus_set_kgradient)
     int kg_n = 0, kg_cap = 0;
     int* kg_shift = nullptr;     // [n][3]
@@ -362,6 +369,32 @@ int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double
     if (h->split && fuse) {
         launch_split(h, in, G, Hee, field, nbatch);
         h->launches++;
+        CU(h, cudaGetLastError());
+        prof_end(h, 0, e0);
+        return EDUS_OK;
+    }
+    if (h->use3 && h->nO == 0) {
+        // rows (k -> R, axis 1), columns (axis 0 both ways + pointwise), rows (R -> k)
+        const int planes = h->P * nbatch;
+        const int N0 = h->N[0], N1 = h->N[1];
+        const long long bs = (long long)h->S;
+        dim3 gr(planes, N0 / h->p3.Rc), gc(planes, N1 / h->p3.Cc), gi(planes * (c ? 2 : 1), N0 / h->p3.Rc);
+        const size_t smr = (size_t)h->p3.Rc * N1 * sizeof(double2);
+        const size_t smc = (size_t)N0 * h->p3.Cc * sizeof(double2) * (c ? 2 : 1);
+        plane3_rows_kernel<true, 256><<<gr, 128, smr, h->stream>>>(in, in_bstride, h->s3a, bs, h->P, h->p3.rows, 1,
+                                                                   h->roots, in, h->s3a);
+        if (c)
+            plane3_cols_kernel<true, 256><<<gc, 128, smc, h->stream>>>(
+                h->s3a, bs, h->s3g, h->s3h, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->p3.cols,
+                h->p3.Cc, h->nb, 1.0 / h->Nk, h->hpos, h->hval, nS);
+        else
+            plane3_cols_kernel<false, 256><<<gc, 128, smc, h->stream>>>(
+                h->s3a, bs, h->s3g, h->s3h, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->p3.cols,
+                h->p3.Cc, h->nb, 1.0 / h->Nk, h->hpos, h->hval, 0);
+        plane3_rows_kernel<false, 256><<<gi, 128, smr, h->stream>>>(h->s3g, bs, G, out_bstride, h->P, h->p3.rows,
+                                                                    c ? 2 : 1, h->roots, h->s3h, Hee);
+        h->launches += 3;
+        if (kmode) launch_kgrad();
         CU(h, cudaGetLastError());
         prof_end(h, 0, e0);
         return EDUS_OK;
@@ -1078,6 +1111,25 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     TRY_ALLOC(h->rpos, rpos.size() * sizeof(double));
     TRY_ALLOC(h->field, (size_t)h->chunk * 4 * h->B * sizeof(StageField));
     if (h->plane_cfg.persist && d.coulomb) TRY_ALLOC(h->plane_scratch, (size_t)h->plane_grid * h->Nk * sizeof(double2));
+    {
+        // few band-pair planes on a 2-D grid: spread each plane over CTAs
+        int nsm = 0;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d.device);
+        const int planes = h->P * h->B;
+        if (d.precision == EDUS_PREC_FP64 && h->N[2] == 1 && h->N[1] > 1 && h->Nk >= 1024 && planes < nsm) {
+            const int Rc = divisor_upto(h->N[0], std::max(1, planes * h->N[0] / nsm));
+            const int Cc = divisor_upto(h->N[1], std::max(1, planes * h->N[1] / nsm));
+            h->p3 = plane3_plan(h->plan, Rc, Cc);
+            TRY_ALLOC(h->s3a, SBb);
+            TRY_ALLOC(h->s3g, SBb);
+            if (d.coulomb) TRY_ALLOC(h->s3h, SBb);
+            if ((rc = set_smem(h, plane3_rows_kernel<true, 256>, Rc * h->N[1] * (int)sizeof(double2)))) return bail(rc);
+            if ((rc = set_smem(h, plane3_rows_kernel<false, 256>, Rc * h->N[1] * (int)sizeof(double2)))) return bail(rc);
+            if ((rc = set_smem(h, plane3_cols_kernel<true, 256>, 2 * h->N[0] * Cc * (int)sizeof(double2)))) return bail(rc);
+            if ((rc = set_smem(h, plane3_cols_kernel<false, 256>, h->N[0] * Cc * (int)sizeof(double2)))) return bail(rc);
+            h->use3 = true;
+        }
+    }
     TRY_ALLOC(h->popbuf, h->nb * sizeof(double));
     TRY_ALLOC(h->flag, sizeof(int));
     if (cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream) != cudaSuccess)
