@@ -231,9 +231,9 @@ def run_ours(args, rank, world, local_rank):
     comm_avg = comm_ms / max(comm_n, 1)
     peak, peak_kind = measured_peaks()
     # the kernels this workload runs: the persistent plane kernel and, for
-    # HSEX with 12..24 bands, the TMA-fed commutator
+    # HSEX with 12..24 bands, the warp-specialised TMA-fed commutator
     plane_name = "plane_rhs_persist_kernel"
-    comm_name = "commutator_pipe_kernel" if (cfg.coulomb and 12 <= model.nb <= 24) else "commutator_mma_kernel"
+    comm_name = "commutator_ws_kernel" if (cfg.coulomb and 12 <= model.nb <= 24) else "commutator_mma_kernel"
     dominant = plane_name if plane_ms >= comm_ms else comm_name
     if dominant == plane_name:
         ach = plane_launch_B / (plane_avg / 1e3) / 1e9

@@ -15,7 +15,7 @@
 #include "../../include/edus_gpu.h"
 #include "kernels.cuh"
 #include "packed_kernels.cuh"
-#include "comm_pipe.cuh"
+#include "comm_ws.cuh"
 #include "split_kernels.cuh"
 #include "plane3.cuh"
 #include <cudaTypedefs.h>
@@ -77,10 +77,12 @@ struct edus_handle {
     int nO = 0, nO_cap = 0;
     // position (digit-reversed plane order) of each frequency index, per axis
     std::vector<int> posof[3];
-    // pipelined commutator of the fused path (12 <= nb <= 24) and its
-    // tensor maps, one per (array, batch count)
-    bool comm_pipe = false;
-    int pipe_grid = 0;
+    // warp-specialised TMA commutator of the fused path (12 <= nb <= 24):
+    // CTAs per launch, and its tensor maps keyed by (array, 2 * batch count +
+    // box kind): kind 0 the dense box, kind 1 the zero-padded box of the
+    // product operands
+    bool comm_ws = false;
+    int ws_grid = 0;
     std::map<std::pair<const void*, int>, CUtensorMap> tmaps;
     // split-precision form (EDUS_PREC_SPLIT32): anchor rho_ref and its FP64 terms
     bool split = false, anchored = false;
@@ -438,18 +440,23 @@ PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
 }
 
 // The [nbatch][P][Nk] complex array at `base` as the 4-D tensor
-// {2 Nk, nb, nb, nbatch} of doubles, box {2 TK, nb, nb, 1}.
-const CUtensorMap* pipe_map(edus_handle* h, const void* base, int nbatch) {
-    const auto key = std::make_pair(base, nbatch);
+// {2 Nk, nb, nb, nbatch} of doubles, box {2 TK, nb, nb, 1} (padded = false)
+// or {2 TK, nbp + 1, nbp, 1} (padded = true: the copy zero-fills the margin).
+const CUtensorMap* operand_map(edus_handle* h, const void* base, int nbatch, bool padded) {
+    const auto key = std::make_pair(base, 2 * nbatch + (padded ? 1 : 0));
     auto it = h->tmaps.find(key);
     if (it != h->tmaps.end()) return &it->second;
     PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
     if (!enc) return nullptr;
-    const PipeGeom g = pipe_geometry(h->nb);
+    const WsGeom g = ws_geometry(h->nb);
     const cuuint64_t nb = (cuuint64_t)h->nb, Nk = (cuuint64_t)h->Nk;
     const cuuint64_t dims[4] = {2 * Nk, nb, nb, (cuuint64_t)nbatch};
     const cuuint64_t strides[3] = {Nk * 16, nb * Nk * 16, nb * nb * Nk * 16};
-    const cuuint32_t box[4] = {(cuuint32_t)(2 * g.TK), (cuuint32_t)nb, (cuuint32_t)nb, 1};
+    cuuint32_t box[4] = {(cuuint32_t)(2 * g.TK), (cuuint32_t)nb, (cuuint32_t)nb, 1};
+    if (padded) {
+        box[1] = (cuuint32_t)g.W;
+        box[2] = (cuuint32_t)g.nbp;
+    }
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     CUtensorMap m;
     const CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(base), dims, strides, box, estr,
@@ -460,22 +467,22 @@ const CUtensorMap* pipe_map(edus_handle* h, const void* base, int nbatch) {
 }
 
 template <int MODE>
-int launch_pipe(edus_handle* h, const StageArgs& a, int nbatch) {
-    const PipeGeom g = pipe_geometry(h->nb);
+int launch_ws(edus_handle* h, const StageArgs& a, int nbatch) {
+    const WsGeom g = ws_geometry(h->nb);
     const int ntiles = ((h->Nk + g.TK - 1) / g.TK) * nbatch;
-    const int grid = std::min(ntiles, h->pipe_grid);
-    PipeMaps maps;
+    const int grid = std::min(ntiles, h->ws_grid);
+    OperandMaps maps;
     const void* src[5] = {a.Hee, a.rho, a.G, a.y ? (const void*)a.y : (const void*)a.G,
                           a.acc ? (const void*)a.acc : (const void*)a.G};
     for (int i = 0; i < 5; ++i) {
-        const CUtensorMap* m = pipe_map(h, src[i], nbatch);
+        const CUtensorMap* m = operand_map(h, src[i], nbatch, i < 2);
         if (!m) return fail(h, EDUS_ERR_CUDA, "cuTensorMapEncodeTiled failed for a commutator operand");
         maps.m[i] = *m;
     }
     if (g.tiles == 3)
-        commutator_pipe_kernel<MODE, 2, 576><<<grid, 576, g.smem, h->stream>>>(a, nbatch, maps, h->flag);
+        commutator_ws_kernel<MODE, 3><<<grid, g.threads, g.smem, h->stream>>>(a, nbatch, maps, h->flag);
     else
-        commutator_pipe_kernel<MODE, 2, 256><<<grid, 256, g.smem, h->stream>>>(a, nbatch, maps, h->flag);
+        commutator_ws_kernel<MODE, 2><<<grid, g.threads, g.smem, h->stream>>>(a, nbatch, maps, h->flag);
     return EDUS_OK;
 }
 
@@ -485,9 +492,9 @@ int launch_comm_mode(edus_handle* h, const StageArgs& a, int nbatch, bool fuse) 
     cudaEvent_t e0;
     prof_begin(h, &e0);
     const bool fh = fuse && h->d.coulomb && (h->nS > 0 || h->split);
-    if (fh && h->comm_pipe) {
+    if (fh && h->comm_ws) {
         int rc;
-        if ((rc = launch_pipe<MODE>(h, a, nbatch))) return rc;
+        if ((rc = launch_ws<MODE>(h, a, nbatch))) return rc;
     } else if (h->comm_mma) {
         if (fh)
             commutator_mma_kernel<MODE, true, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
@@ -1050,24 +1057,26 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     if ((rc = set_smem(h, commutator_mma_kernel<M, true, true>, smem_cmax))) return bail(rc);
     SETC(MODE_RHS) SETC(MODE_RK1) SETC(MODE_RK2) SETC(MODE_RK3) SETC(MODE_RK4) SETC(MODE_AB)
 #undef SETC
-    if (d.coulomb && pipe_supported(h->nb)) {
-        const PipeGeom pg = pipe_geometry(h->nb);
-        if ((int)pg.smem <= dev_smem) {
-#define SETP(M)                                                                                              \
-    if ((rc = set_smem(h, commutator_pipe_kernel<M, 2, 576>, (int)pg.smem))) return bail(rc);            \
-    if ((rc = set_smem(h, commutator_pipe_kernel<M, 2, 256>, (int)pg.smem))) return bail(rc);
-            SETP(MODE_RHS) SETP(MODE_RK1) SETP(MODE_RK2) SETP(MODE_RK3) SETP(MODE_RK4) SETP(MODE_AB)
-#undef SETP
+    if (d.coulomb && ws_supported(h->nb) && tensor_map_encoder()) {
+        const WsGeom wg = ws_geometry(h->nb);
+        if ((int)wg.smem <= dev_smem) {
+#define SETW(M)                                                                                           \
+    if ((rc = set_smem(h, commutator_ws_kernel<M, 3>, (int)wg.smem))) return bail(rc);       \
+    if ((rc = set_smem(h, commutator_ws_kernel<M, 2>, (int)wg.smem))) return bail(rc);
+            SETW(MODE_RHS) SETW(MODE_RK1) SETW(MODE_RK2) SETW(MODE_RK3) SETW(MODE_RK4) SETW(MODE_AB)
+#undef SETW
             int per_sm = 0;
-            if (pg.tiles == 3)
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commutator_pipe_kernel<MODE_RK2, 2, 576>, 576, pg.smem);
+            if (wg.tiles == 3)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commutator_ws_kernel<MODE_RK2, 3>,
+                                                              wg.threads, wg.smem);
             else
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commutator_pipe_kernel<MODE_RK2, 2, 256>, 256, pg.smem);
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commutator_ws_kernel<MODE_RK2, 2>,
+                                                              wg.threads, wg.smem);
             int nsm = 0;
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d.device);
-            if (per_sm > 0 && nsm > 0 && tensor_map_encoder()) {
-                h->comm_pipe = true;
-                h->pipe_grid = per_sm * nsm;
+            if (per_sm > 0 && nsm > 0) {
+                h->comm_ws = true;
+                h->ws_grid = per_sm * nsm;
             }
         }
     }
@@ -1978,7 +1987,7 @@ int edus_autotune(edus_handle* h, int* plane_threads, int* comm_tensor) {
     // commutator: the CUDA-core against the tensor-core kernel (the TMA kernel
     // of the fused HSEX path has one geometry)
     {
-        const bool fused = h->d.coulomb && (h->nS > 0 || h->split) && h->comm_pipe;
+        const bool fused = h->d.coulomb && (h->nS > 0 || h->split) && h->comm_ws;
         if (!fused) {
             StageArgs a = base_args(h);
             a.rho = h->y;

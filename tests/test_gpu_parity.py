@@ -113,9 +113,12 @@ def test_steps_parity(pkg, po, tmp_path, solver, order, coulomb):
         assert s.time == pytest.approx(o.time, rel=0, abs=1e-12)
 
 
+# the fused HSEX commutator for 12 <= nb <= 24: 8x8 tiles in 2x2 (nb 13) and 3x3
+# (nb 19, 24) blocks; an odd k count (35) leaves the last tile one k point short
+@pytest.mark.parametrize("nb,grid", [(13, (8, 9, 1)), (19, (7, 5, 1)), (24, (6, 4, 1))])
 @pytest.mark.parametrize("solver,order", [("RK", 4), ("AB", 4)])
-def test_steps_parity_mma(pkg, po, tmp_path, solver, order):
-    inp = model_input(pkg, tmp_path, f"stm_{solver}{order}", (8, 9, 1), nb=13, coulomb=True, solver=solver,
+def test_steps_parity_mma(pkg, po, tmp_path, solver, order, nb, grid):
+    inp = model_input(pkg, tmp_path, f"stm_{solver}{order}_{nb}", grid, nb=nb, coulomb=True, solver=solver,
                       order=order, dt=0.01)
     cfg, o, s = make_pair(pkg, po, inp, batch=2)
     for chunk in (1, 4, 10):
