@@ -257,6 +257,20 @@ struct Dft<10, S, C> : DftComposite<2, 5, S, C> {};
 template <int S, typename C>
 struct Dft<12, S, C> : DftComposite<4, 3, S, C> {};
 
+// w[d] = w1^d (conjugated when CONJ), d = 1 .. R-1, by binary powers: each
+// entry is at most three products from w1
+template <int R, bool CONJ, typename C>
+__device__ __forceinline__ void twiddle_powers(C* w, C w1) {
+    if (CONJ) w1.y = -w1.y;
+    w[1] = w1;
+#pragma unroll
+    for (int d = 2; d < R; ++d) {
+        const int hi = (d & 1) ? d - 1 : d / 2;  // d = hi + lo with lo = 1 (odd d) or hi (even d)
+        const int lo = d - hi;
+        w[d] = cmul(w[hi], w[lo]);
+    }
+}
+
 // One radix-R stage over every line of axis `ax` of the NBUF planes that
 // start at `buf[0]`, `buf[0] + bufstride`, ...  DIF when FWD, DIT otherwise.
 template <int R, bool FWD, int NBUF, typename C>
@@ -289,20 +303,17 @@ __device__ __forceinline__ void stage_R(C* buf, int bufstride, int Nk, const Axi
             if (FWD) {
                 Dft<R, S, C>::run(v, root, n);
                 if (a != 0) {
+                    C w[R];
+                    twiddle_powers<R, false>(w, ldroot<C>(&root[a * tw_step]));
 #pragma unroll
-                    for (int d = 1; d < R; ++d) {
-                        const C w = ldroot<C>(&root[a * d * tw_step]);
-                        v[d] = cmul(v[d], w);
-                    }
+                    for (int d = 1; d < R; ++d) v[d] = cmul(v[d], w[d]);
                 }
             } else {
                 if (a != 0) {
+                    C w[R];
+                    twiddle_powers<R, true>(w, ldroot<C>(&root[a * tw_step]));
 #pragma unroll
-                    for (int d = 1; d < R; ++d) {
-                        C w = ldroot<C>(&root[a * d * tw_step]);
-                        w.y = -w.y;
-                        v[d] = cmul(v[d], w);
-                    }
+                    for (int d = 1; d < R; ++d) v[d] = cmul(v[d], w[d]);
                 }
                 Dft<R, S, C>::run(v, root, n);
             }
