@@ -13,12 +13,15 @@ each step whose time t has int(round(t/dt)) % printresolution_pulse == 0
     Time.txt                t (a.u.)
     Laser.txt               E(t), Cartesian (a.u.)
     Laser_A.txt             the vector potential, integrated by Simpson's rule
-                            from one printed time to the next (Laser.cpp:136-151)
+                            from one printed time to the next (Laser.cpp:136-151);
+                            in the Peierls gauge every stage time is a step of the
+                            same integrator, as there the source term requests A too
     Population.txt          Bloch populations, holes of the filled bands
     Population_wannier.txt  Wannier populations
     Velocity.txt            re, im of the x, y, z velocity
 
-The observables are computed on the GPU (edus_observables).  Differences from
+The observables are computed on the GPU (edus_observables; in the Peierls gauge
+of the state rho(R) e^{-iA.R}, Simulation.cpp:447-449, 593-595).  Differences from
 the reference: the vector potential integrates the total field of all lasers
 (the reference's accumulator is a function-static shared by every laser, which
 only agrees for a single laser); output.h5 is not written.
@@ -64,11 +67,14 @@ def run(input_path: str, outdir: str, device: int = 0) -> int:
         while it < nsteps:
             if int(round(t / dt)) % pr == 0:
                 E = s.efield(t)
-                dT = t - t_prev
-                if dT >= 1e-7:
-                    E1, E2 = s.efield(t_prev), s.efield(t_prev + dT / 2.0)
-                    A = [A[d] - dT / 6.0 * (E1[d] + 4.0 * E2[d] + E[d]) for d in range(3)]
-                    t_prev = t
+                if cfg.peierls:
+                    A = list(s.vector_potential(t))
+                else:
+                    dT = t - t_prev
+                    if dT >= 1e-7:
+                        E1, E2 = s.efield(t_prev), s.efield(t_prev + dT / 2.0)
+                        A = [A[d] - dT / 6.0 * (E1[d] + 4.0 * E2[d] + E[d]) for d in range(3)]
+                        t_prev = t
                 pb, pw, v = s.observables(0, cfg.filledbands)
                 files["Time"].write(f"{t:g}\n")
                 files["Laser"].write("".join(f"{x:24.15g}" for x in E) + "\n")

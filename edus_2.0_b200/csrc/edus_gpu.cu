@@ -83,6 +83,12 @@ struct edus_handle {
     // product operands
     bool comm_ws = false;
     int ws_grid = 0;
+    // Peierls gauge (edus_set_peierls): per-axis phase tables of the stage
+    // ([B][ntab]) and each solve's vector-potential integrator (A, last time)
+    bool peierls = false;
+    double2* ptab = nullptr;
+    int ntab = 0;
+    std::vector<double> Avec, Aprev;
     std::map<std::pair<const void*, int>, CUtensorMap> tmaps;
     // split-precision form (EDUS_PREC_SPLIT32): anchor rho_ref and its FP64 terms
     bool split = false, anchored = false;
@@ -209,6 +215,34 @@ void field_at(const std::vector<edus_laser>& ls, const double A[9], double t, St
     }
     for (int d = 0; d < 3; ++d) f.E[d] = E[d];
     for (int c = 0; c < 3; ++c) f.g[c] = A[0 * 3 + c] * E[0] + A[1 * 3 + c] * E[1] + A[2 * 3 + c] * E[2];
+    for (int c = 0; c < 3; ++c) f.ga[c] = 0.0;
+}
+
+// Laser::VectorPotential (Laser.cpp:136-151) for solve b, advanced to t:
+// when t - t_prev >= 1e-7, A -= (t - t_prev)/6 (E(t_prev) + 4 E(mid) + E(t)) and
+// t_prev = t.  The reference keeps A and t_prev in function statics, starting
+// from 0 and 0, shared by all lasers; here each solve integrates the total
+// field of its lasers (the same for one laser).
+void advance_vecpot(edus_handle* h, int b, double t) {
+    const double dT = t - h->Aprev[b];
+    if (dT < 1.e-07) return;
+    StageField f1, f2, f3;
+    field_at(h->lasers[b], h->A, h->Aprev[b], f1);
+    field_at(h->lasers[b], h->A, h->Aprev[b] + dT / 2., f2);
+    field_at(h->lasers[b], h->A, t, f3);
+    for (int d = 0; d < 3; ++d) h->Avec[3 * b + d] -= dT / 6. * (f1.E[d] + 4. * f2.E[d] + f3.E[d]);
+    h->Aprev[b] = t;
+}
+
+// Peierls gauge at stage time t of solve b: no gradient term (g = 0) and
+// ga = A^T A(t), so that A(t).R = ga . R_crys (Simulation.cpp:876-899)
+void peierls_field(edus_handle* h, int b, double t, StageField& f) {
+    advance_vecpot(h, b, t);
+    for (int c = 0; c < 3; ++c) {
+        f.g[c] = 0.0;
+        f.ga[c] = h->A[0 * 3 + c] * h->Avec[3 * b] + h->A[1 * 3 + c] * h->Avec[3 * b + 1] +
+                  h->A[2 * 3 + c] * h->Avec[3 * b + 2];
+    }
 }
 
 cudaEvent_t prof_event(edus_handle* h) {
@@ -293,19 +327,22 @@ __global__ void kgradient_kernel(const double2* __restrict__ rho, long long in_b
 
 template <bool COUL, int MASK, int MAXT>
 void launch_plane_variant(edus_handle* h, dim3 grid, const double2* in, long long in_bstride, double2* G,
-                          double2* Hee, long long out_bstride, const StageField* field, int nS) {
+                          double2* Hee, long long out_bstride, const StageField* field, int nS,
+                          const double2* ptab = nullptr) {
     plane_rhs_kernel<COUL, MASK, MAXT><<<grid, h->plane_cfg.threads, h->smem_plane, h->stream>>>(
         in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
-        1.0 / h->Nk, h->hpos, h->hval, nS);
+        1.0 / h->Nk, h->hpos, h->hval, nS, ptab, h->ntab);
 }
 
 template <bool COUL, int MASK, int MAXT>
 void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long long in_bstride, double2* G,
-                          double2* Hee, long long out_bstride, const StageField* field, int nS) {
+                          double2* Hee, long long out_bstride, const StageField* field, int nS,
+                          const double2* ptab = nullptr) {
     const int grid = std::min(nplanes, h->plane_grid);
     plane_rhs_persist_kernel<COUL, MASK, MAXT><<<grid, h->plane_cfg.threads, h->Nk * sizeof(double2), h->stream>>>(
         in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
-        1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0);
+        1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0, ptab,
+        h->ntab);
 }
 
 // fuse: with HSEX and a sparse model, Hee receives the whole Hamiltonian
@@ -362,6 +399,31 @@ int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double
             in, in_bstride, G, out_bstride, h->kg_shift, h->kg_coef, h->kg_n, field, h->N[0], h->N[1], h->N[2], h->P);
         h->launches++;
     };
+    if (h->peierls) {
+        // Peierls gauge: the stage's phase tables, then H alone (G stays zero)
+        peierls_phase_kernel<<<nbatch, 128, 0, h->stream>>>(field, h->rpos, h->plan, h->ntab, h->ptab);
+        h->launches++;
+        const int np = h->P * nbatch;
+        if (h->plane_cfg.persist) {
+            if (h->plane_cfg.variant == 1) {
+                if (c) launch_plane_persist<true, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+                else launch_plane_persist<false, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+            } else {
+                if (c) launch_plane_persist<true, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+                else launch_plane_persist<false, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+            }
+        } else if (h->plane_cfg.variant == 1) {
+            if (c) launch_plane_variant<true, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+            else launch_plane_variant<false, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+        } else {
+            if (c) launch_plane_variant<true, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+            else launch_plane_variant<false, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+        }
+        h->launches++;
+        CU(h, cudaGetLastError());
+        prof_end(h, 0, e0);
+        return EDUS_OK;
+    }
     if (kmode && !c) {
         launch_kgrad();
         CU(h, cudaGetLastError());
@@ -491,10 +553,17 @@ int launch_comm_mode(edus_handle* h, const StageArgs& a, int nbatch, bool fuse) 
     dim3 grid((h->Nk + h->TK - 1) / h->TK, nbatch);
     cudaEvent_t e0;
     prof_begin(h, &e0);
-    const bool fh = fuse && h->d.coulomb && (h->nS > 0 || h->split);
+    // fused Hamiltonian: Hee holds the whole H (with HSEX and a sparse model,
+    // and always in the Peierls gauge)
+    const bool fh = fuse && ((h->d.coulomb && (h->nS > 0 || h->split)) || h->peierls);
     if (fh && h->comm_ws) {
         int rc;
         if ((rc = launch_ws<MODE>(h, a, nbatch))) return rc;
+    } else if (fh && !h->d.coulomb) {
+        if (h->comm_mma)
+            commutator_mma_kernel<MODE, false, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
+        else
+            commutator_kernel<MODE, false, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
     } else if (h->comm_mma) {
         if (fh)
             commutator_mma_kernel<MODE, true, true><<<grid, h->comm_threads, h->smem_comm, h->stream>>>(a);
@@ -780,6 +849,29 @@ int anchor_split(edus_handle* h) {
 // Re (U^dagger rho U)_nn, the Wannier populations Re rho_nn and tr(v_d rho),
 // accumulated in acc[0..nb) (Bloch), acc[nb..2nb) (Wannier), acc[2nb..2nb+6)
 // (re, im of d = 0, 1, 2).  Shared memory: rho_k and U_k, [n][m].
+// Peierls gauge, observables (Simulation.cpp:447-449, 593-595): the state
+// that the populations and the velocity see is rho(R) e^{-iA.R} back in k,
+// one plane per CTA: dst = FFT_{+1}(FFT_{-1}(src) e^{-iA.R} / Nk).
+template <int MASK, int MAXT>
+__global__ void __launch_bounds__(MAXT) peierls_shift_kernel(const double2* __restrict__ src, double2* __restrict__ dst,
+                                                             const double2* __restrict__ tb,
+                                                             const double2* __restrict__ roots, PlanePlan pl,
+                                                             double inv_nk) {
+    extern __shared__ double2 xs[];
+    const int Nk = pl.Nk;
+    const long long off = (long long)blockIdx.x * Nk;
+    for (int i = threadIdx.x; i < Nk; i += blockDim.x) xs[i] = __ldg(&src[off + i]);
+    __syncthreads();
+    plane_forward<1, MASK>(xs, 0, pl, roots);
+    for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
+        const double2 e = peierls_phase_at(tb, pl, j);
+        xs[j] = cmul(cscale(xs[j], inv_nk), make_double2(e.x, -e.y));
+    }
+    __syncthreads();
+    plane_inverse<1, MASK>(xs, 0, pl, roots);
+    for (int i = threadIdx.x; i < Nk; i += blockDim.x) dst[off + i] = xs[i];
+}
+
 __global__ void observables_kernel(const double2* __restrict__ rho, const double2* __restrict__ U,
                                    const double2* __restrict__ v0, const double2* __restrict__ v1,
                                    const double2* __restrict__ v2, int Nk, int nb, double* __restrict__ acc) {
@@ -1045,6 +1137,9 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     if ((rc = set_smem(h, plane_rhs_kernel<false, kRadix89, 768>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_to_R_kernel<kRadixAll, 256>, h->Nk * (int)sizeof(double2)))) return bail(rc);
     if ((rc = set_smem(h, observables_kernel, 2 * h->P * (int)sizeof(double2)))) return bail(rc);
+    if (h->Nk * (int)sizeof(double2) <= dev_smem &&
+        (rc = set_smem(h, peierls_shift_kernel<kRadixAll, 256>, h->Nk * (int)sizeof(double2))))
+        return bail(rc);
     if ((rc = set_smem(h, kgradient_kernel, 4096 * (int)(sizeof(double) + 3 * sizeof(int))))) return bail(rc);
     // the attribute covers both commutator variants, which the autotuner may swap
     const int smem_cmax = (int)std::max(comm_geometry(h->nb).smem, mma_geometry(h->nb).smem);
@@ -1054,7 +1149,9 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     if ((rc = set_smem(h, commutator_mma_kernel<M, true>, smem_cmax))) return bail(rc);       \
     if ((rc = set_smem(h, commutator_mma_kernel<M, false>, smem_cmax))) return bail(rc);     \
     if ((rc = set_smem(h, commutator_kernel<M, true, true>, smem_cmax))) return bail(rc);     \
-    if ((rc = set_smem(h, commutator_mma_kernel<M, true, true>, smem_cmax))) return bail(rc);
+    if ((rc = set_smem(h, commutator_mma_kernel<M, true, true>, smem_cmax))) return bail(rc);      \
+    if ((rc = set_smem(h, commutator_kernel<M, false, true>, smem_cmax))) return bail(rc);     \
+    if ((rc = set_smem(h, commutator_mma_kernel<M, false, true>, smem_cmax))) return bail(rc);
     SETC(MODE_RHS) SETC(MODE_RK1) SETC(MODE_RK2) SETC(MODE_RK3) SETC(MODE_RK4) SETC(MODE_AB)
 #undef SETC
     if (d.coulomb && ws_supported(h->nb) && tensor_map_encoder()) {
@@ -1454,6 +1551,52 @@ int edus_set_kgradient(edus_handle* h, int n, const int* shift, const double* b,
     return EDUS_OK;
 }
 
+int edus_set_peierls(edus_handle* h, int on) {
+    if (!h) return EDUS_ERR_ARG;
+    CU(h, cudaSetDevice(h->d.device));
+    CU(h, cudaStreamSynchronize(h->stream));
+    if (!on) {
+        h->peierls = false;
+        return EDUS_OK;
+    }
+    if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "edus_upload_model must be called first");
+    if (h->packed || h->split) return fail(h, EDUS_ERR_UNSUPPORTED, "the Peierls gauge is implemented for the FP64 form");
+    if (h->per_solve) return fail(h, EDUS_ERR_UNSUPPORTED, "the Peierls gauge needs one model for all solves");
+    if (h->nO > 0) return fail(h, EDUS_ERR_UNSUPPORTED, "the Peierls gauge does not combine with a Fock override");
+    if (h->Nk * sizeof(double2) > (size_t)device_smem_optin(h->d.device))
+        return fail(h, EDUS_ERR_UNSUPPORTED, "the Peierls gauge needs a plane (16 Nk bytes) in shared memory");
+    int rc;
+    if (!h->d.coulomb && h->nS == 0 && (rc = build_sparse_model(h))) return rc;
+    if (h->nS == 0)
+        return fail(h, EDUS_ERR_UNSUPPORTED,
+                    "the Peierls gauge needs H0(R) and xi(R) on at most 4096 lattice vectors");
+    const size_t SBb = h->S * sizeof(double2) * h->B;
+    if (!h->Hee && (rc = dalloc(h, (void**)&h->Hee, SBb))) return rc;
+    if (!h->ptab) {
+        h->ntab = h->N[0] + h->N[1] + h->N[2];
+        if ((rc = dalloc(h, (void**)&h->ptab, (size_t)h->B * h->ntab * sizeof(double2)))) return rc;
+    }
+    // no gradient term: the commutators read G = 0
+    CU(h, cudaMemsetAsync(h->G, 0, SBb, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    h->Avec.assign(3 * (size_t)h->B, 0.0);
+    h->Aprev.assign(h->B, 0.0);
+    h->peierls = true;
+    return EDUS_OK;
+}
+
+int edus_vector_potential(edus_handle* h, int b, double t, double* A) {
+    if (!h || !A) return EDUS_ERR_ARG;
+    if (b < 0 || b >= h->B) return fail(h, EDUS_ERR_ARG, "solve index out of range");
+    if ((int)h->Aprev.size() != h->B) {
+        h->Avec.assign(3 * (size_t)h->B, 0.0);
+        h->Aprev.assign(h->B, 0.0);
+    }
+    advance_vecpot(h, b, t);
+    for (int d = 0; d < 3; ++d) A[d] = h->Avec[3 * b + d];
+    return EDUS_OK;
+}
+
 int edus_upload_observables(edus_handle* h, const double* U_k, const double* vel_k) {
     if (!h || (!U_k && !vel_k)) return EDUS_ERR_ARG;
     CU(h, cudaSetDevice(h->d.device));
@@ -1488,9 +1631,23 @@ int edus_observables(edus_handle* h, int b, int filled, double* pop_bloch, doubl
     CU(h, cudaSetDevice(h->d.device));
     if (h->packed && (rc = unpack_state(h, b))) return rc;
     const int nacc = 2 * h->nb + 6;
+    const double2* rho = h->y + (size_t)b * h->S;
+    if (h->peierls) {
+        // the gauge-shifted state at the handle's time, in the transpose buffer
+        StageField f;
+        field_at(h->lasers[b], h->A, h->t, f);
+        peierls_field(h, b, h->t, f);
+        CU(h, cudaMemcpyAsync(h->field, &f, sizeof(StageField), cudaMemcpyHostToDevice, h->stream));
+        peierls_phase_kernel<<<1, 128, 0, h->stream>>>(h->field, h->rpos, h->plan, h->ntab, h->ptab);
+        peierls_shift_kernel<kRadixAll, 256><<<h->P, 256, h->Nk * sizeof(double2), h->stream>>>(
+            rho, h->stage, h->ptab, h->roots, h->plan, 1.0 / h->Nk);
+        h->launches += 2;
+        CU(h, cudaGetLastError());
+        rho = h->stage;
+    }
     CU(h, cudaMemsetAsync(h->obsacc, 0, nacc * sizeof(double), h->stream));
     observables_kernel<<<h->Nk, 128, 2 * h->P * sizeof(double2), h->stream>>>(
-        h->y + (size_t)b * h->S, pop_bloch ? h->obsU : nullptr, vel ? h->obsV[0] : nullptr, h->obsV[1], h->obsV[2],
+        rho, pop_bloch ? h->obsU : nullptr, vel ? h->obsV[0] : nullptr, h->obsV[1], h->obsV[2],
         h->Nk, h->nb, h->obsacc);
     h->launches++;
     CU(h, cudaGetLastError());
@@ -1642,6 +1799,7 @@ int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k) {
     CU(h, cudaEventSynchronize(h->field_ev[0]));
     field_at(h->lasers[0], h->A, t, h->field_host[0][0]);
     if (h->kg_n > 0) h->field_host[0][0].g[0] = h->field_host[0][0].g[1] = h->field_host[0][0].g[2] = 0.0;
+    if (h->peierls) peierls_field(h, 0, t, h->field_host[0][0]);
     CU(h, cudaMemcpyAsync(h->field, h->field_host[0], sizeof(StageField), cudaMemcpyHostToDevice, h->stream));
     CU(h, cudaEventRecord(h->field_ev[0], h->stream));
     dim3 tb(32, 8), tg((h->Nk + 31) / 32, (h->P + 31) / 32);
@@ -1677,6 +1835,7 @@ static void fill_field_table(edus_handle* h, int cnt, StageField* tab) {
                 StageField& f = tab[((size_t)i * nst + s) * h->B + b];
                 field_at(h->lasers[b], h->A, ts[s], f);
                 if (h->kg_n > 0) f.g[0] = f.g[1] = f.g[2] = 0.0;  // the gradient is the k stencil
+                if (h->peierls) peierls_field(h, b, ts[s], f);
             }
         t += dt;
     }

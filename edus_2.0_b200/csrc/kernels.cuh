@@ -20,7 +20,49 @@ namespace edus {
 struct StageField {
     double E[3];
     double g[3];
+    double ga[3];  // Peierls gauge: A.R = ga . R_crys with A(t) the vector potential
 };
+
+// Peierls phases of one stage, per solve b and axis: tab[b * ntab + rposoff_d + q]
+// = exp(i ga_d R_d(q)), R_d(q) the Gamma-centred coordinate of position q, so
+// that exp(i A.R) = tab[q0] tab[q1] tab[q2] (Simulation.cpp:876-899).
+__global__ void peierls_phase_kernel(const StageField* __restrict__ field, const double* __restrict__ rpos,
+                                     PlanePlan pl, int ntab, double2* __restrict__ tab) {
+    const StageField F = field[blockIdx.x];
+    for (int d = 0; d < 3; ++d) {
+        const int n = pl.ax[d].n, off = pl.ax[d].rposoff;
+        for (int q = threadIdx.x; q < n; q += blockDim.x) {
+            double sn, cs;
+            sincos(F.ga[d] * rpos[off + q], &sn, &cs);
+            tab[(long long)blockIdx.x * ntab + off + q] = make_double2(cs, sn);
+        }
+    }
+}
+
+// exp(i A.R) at plane position j from the per-axis tables of one solve
+__device__ __forceinline__ double2 peierls_phase_at(const double2* __restrict__ tb, const PlanePlan& pl, int j) {
+    const int t = fdiv(j, pl.fd_n2);
+    const int q2 = j - t * pl.ax[2].n;
+    const int q0 = fdiv(t, pl.fd_n1);
+    const int q1 = t - q0 * pl.ax[1].n;
+    return cmul(cmul(__ldg(&tb[pl.ax[0].rposoff + q0]), __ldg(&tb[pl.ax[1].rposoff + q1])),
+                __ldg(&tb[pl.ax[2].rposoff + q2]));
+}
+
+// Peierls gauge, pointwise: rho(R) -> -W (rho(R) exp(-i A.R) - rho0) exp(+i A.R)
+// in place (X holds Nk rho(R)); the gauge-shifted rho enters the self-energy
+// and the Hamiltonian leaves with the phase (Functional_SourceTerm.hpp:31-44).
+__device__ __forceinline__ void peierls_selfenergy(double2* X, const double2* __restrict__ r0p,
+                                                   const double* __restrict__ wp, const double2* __restrict__ tb,
+                                                   const PlanePlan& pl, double inv_nk) {
+    for (int j = threadIdx.x; j < pl.Nk; j += blockDim.x) {
+        const double2 e = peierls_phase_at(tb, pl, j);
+        const double2 a = cmul(cscale(X[j], inv_nk), make_double2(e.x, -e.y));
+        const double2 r0 = __ldg(&r0p[j]);
+        const double wv = __ldg(&wp[j]);
+        X[j] = cmul(make_double2(-wv * (a.x - r0.x), -wv * (a.y - r0.y)), e);
+    }
+}
 
 // Fused Hamiltonian (HSEX only): the model part H0(R) + sum_d E_d xi_d(R) is
 // added to the self-energy plane in R before its transform, as the reference
@@ -29,23 +71,28 @@ struct StageField {
 // H0(R) and xi(R) of a tight-binding model live on a few lattice vectors: nS
 // positions hpos[s] (digit-reversed plane order) with values
 // hval[(d * P + p) * nS + s], d = 0 for H0 and 1 + axis for xi.
+// In the Peierls gauge (tb != nullptr) the model term is added times its
+// phase exp(i A.R) (Simulation.cpp:876-899); pl is read only then.
 __device__ __forceinline__ void add_model_R(double2* X, const int* __restrict__ hpos,
                                             const double2* __restrict__ hval, int nS, int p, int P,
-                                            const StageField& F) {
+                                            const StageField& F, const double2* __restrict__ tb = nullptr,
+                                            const PlanePlan* pl = nullptr) {
     for (int s = threadIdx.x; s < nS; s += blockDim.x) {
-        double2 v = X[__ldg(&hpos[s])];
-        const double2 h0 = __ldg(&hval[(long long)p * nS + s]);
-        v.x += h0.x;
-        v.y += h0.y;
+        const int pos = __ldg(&hpos[s]);
+        double2 m = __ldg(&hval[(long long)p * nS + s]);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             if (F.E[d] != 0.0) {
                 const double2 x = __ldg(&hval[((long long)(d + 1) * P + p) * nS + s]);
-                v.x += F.E[d] * x.x;
-                v.y += F.E[d] * x.y;
+                m.x += F.E[d] * x.x;
+                m.y += F.E[d] * x.y;
             }
         }
-        X[__ldg(&hpos[s])] = v;
+        double2 v = X[pos];
+        if (tb) m = cmul(m, peierls_phase_at(tb, *pl, pos));
+        v.x += m.x;
+        v.y += m.y;
+        X[pos] = v;
     }
 }
 
@@ -79,13 +126,40 @@ __global__ void __launch_bounds__(MAXT) plane_rhs_kernel(
     double2* __restrict__ Hee_out, long long batch_stride_out, const double2* __restrict__ rho0p,
     const double* __restrict__ Wp, double2* __restrict__ diag0, const StageField* __restrict__ field,
     const double2* __restrict__ roots, const double* __restrict__ rpos, PlanePlan pl, int nb, double inv_nk,
-    const int* __restrict__ hpos, const double2* __restrict__ hval, int nS) {
+    const int* __restrict__ hpos, const double2* __restrict__ hval, int nS,
+    const double2* __restrict__ ptab = nullptr, int ntab = 0) {
     extern __shared__ double2 smem[];
     const int Nk = pl.Nk;
     double2* X = smem;
     double2* Y = smem + Nk;
     const int p = blockIdx.x;
     const int b = blockIdx.y;
+    if (ptab) {
+        // Peierls gauge: no gradient term; H = (H0 + E.xi + Hee[rho e^{-iA.R}]) e^{iA.R}
+        const double2* tb = ptab + (long long)b * ntab;
+        const StageField F = field[b];
+        double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
+        if (COUL) {
+            const double2* src = rho + (long long)b * batch_stride_in + (long long)p * Nk;
+            for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
+            __syncthreads();
+            plane_forward<1, MASK>(X, 0, pl, roots);
+            const int n = p / nb, m = p - (p / nb) * nb;
+            if (n == m && threadIdx.x == 0) diag0[b * nb + n] = cscale(X[0], inv_nk);
+            __syncthreads();
+            peierls_selfenergy(X, rho0p + (long long)p * Nk, Wp + (long long)p * Nk, tb, pl, inv_nk);
+        } else {
+            for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        if (nS > 0) {
+            add_model_R(X, hpos, hval, nS, p, nb * nb, F, tb, &pl);
+            __syncthreads();
+        }
+        plane_inverse<1, MASK>(X, 0, pl, roots);
+        for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = X[i];
+        return;
+    }
     const double2* src = rho + (long long)b * batch_stride_in + (long long)p * Nk;
     for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
     __syncthreads();
@@ -147,7 +221,8 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     const double* __restrict__ Wp, double2* __restrict__ diag0, const StageField* __restrict__ field,
     const double2* __restrict__ roots, const double* __restrict__ rpos, PlanePlan pl, int nb, double inv_nk,
     double2* __restrict__ scratch, int nplanes, const int* __restrict__ hpos, const double2* __restrict__ hval,
-    int nS, const int* __restrict__ opos, const double2* __restrict__ oval, int nO) {
+    int nS, const int* __restrict__ opos, const double2* __restrict__ oval, int nO,
+    const double2* __restrict__ ptab = nullptr, int ntab = 0) {
     extern __shared__ double2 smem[];
     const int Nk = pl.Nk;
     const int P = nb * nb;
@@ -159,6 +234,34 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     const double* rp2 = rpos + pl.ax[2].rposoff;
     for (int w = blockIdx.x; w < nplanes; w += gridDim.x) {
         const int b = w / P, p = w - (w / P) * P;
+        if (ptab) {
+            // Peierls gauge: no gradient term, two transforms (one without
+            // HSEX); H = (H0 + E.xi + Hee[rho e^{-iA.R}]) e^{iA.R}
+            const double2* tb = ptab + (long long)b * ntab;
+            const StageField F = field[b];
+            if (COUL) {
+                const double2* src = rho + (long long)b * batch_stride_in + (long long)p * Nk;
+                for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
+                __syncthreads();
+                plane_forward<1, MASK>(X, 0, pl, roots);
+                const int n = p / nb, m = p - (p / nb) * nb;
+                if (n == m && threadIdx.x == 0) diag0[b * nb + n] = cscale(X[0], inv_nk);
+                __syncthreads();
+                peierls_selfenergy(X, rho0p + (long long)p * Nk, Wp + (long long)p * Nk, tb, pl, inv_nk);
+            } else {
+                for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = make_double2(0.0, 0.0);
+            }
+            __syncthreads();
+            if (nS > 0) {
+                add_model_R(X, hpos, hval, nS, p, P, F, tb, &pl);
+                __syncthreads();
+            }
+            plane_inverse<1, MASK>(X, 0, pl, roots);
+            double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
+            for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = X[i];
+            __syncthreads();  // X is reloaded by the next plane
+            continue;
+        }
         const double2* src = rho + (long long)b * batch_stride_in + (long long)p * Nk;
         for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
         __syncthreads();
@@ -345,7 +448,7 @@ __device__ __forceinline__ void load_stage_inputs(const StageArgs& a, const Stag
                 if (e0) x0[u] = __ldg(&a.xi[0][em]);
                 if (e1) x1[u] = __ldg(&a.xi[1][em]);
                 if (e2) x2[u] = __ldg(&a.xi[2][em]);
-                if (COUL) he[u] = __ldg(&a.Hee[boff + el[u]]);
+                if (COUL || FH) he[u] = __ldg(&a.Hee[boff + el[u]]);
             }
         }
 #pragma unroll
@@ -361,10 +464,8 @@ __device__ __forceinline__ void load_stage_inputs(const StageArgs& a, const Stag
                 if (e0) { hv.x += F.E[0] * x0[u].x; hv.y += F.E[0] * x0[u].y; }
                 if (e1) { hv.x += F.E[1] * x1[u].x; hv.y += F.E[1] * x1[u].y; }
                 if (e2) { hv.x += F.E[2] * x2[u].x; hv.y += F.E[2] * x2[u].y; }
-                if (COUL) {
-                    hv = cadd(hv, he[u]);
-                    if (i == j) hv = cadd(hv, hh[i]);
-                }
+                if (COUL || FH) hv = cadd(hv, he[u]);
+                if (COUL && i == j) hv = cadd(hv, hh[i]);
             }
             store(i, j, kk, hv, rv);
         }

@@ -37,6 +37,7 @@ EXPORTS = [
     "edus_mlp_create", "edus_mlp_destroy", "edus_mlp_last_error", "edus_mlp_param_count", "edus_mlp_set_params",
     "edus_mlp_get_params", "edus_mlp_forward", "edus_mlp_gradients", "edus_mlp_train_step",    "edus_upload_model_solve", "edus_sweep_step", "edus_autotune",
     "edus_upload_observables", "edus_observables", "edus_efield", "edus_set_kgradient",
+    "edus_set_peierls", "edus_vector_potential",
 ]
 
 
@@ -115,6 +116,8 @@ def load_library(path: str | None = None):
     L.edus_set_kgradient.argtypes = [h, ctypes.c_int, P(ctypes.c_int), dp, dp]
     L.edus_observables.argtypes = [h, ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.edus_efield.argtypes = [h, ctypes.c_int, ctypes.c_double, dp]
+    L.edus_set_peierls.argtypes = [h, ctypes.c_int]
+    L.edus_vector_potential.argtypes = [h, ctypes.c_int, ctypes.c_double, dp]
     L.edus_sweep_step.argtypes = [P(h), ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.edus_autotune.argtypes = [h, P(ctypes.c_int), P(ctypes.c_int)]
     ip = P(ctypes.c_int)
@@ -313,6 +316,17 @@ class Solver:
         E = np.empty(3)
         self._check(self._L.edus_efield(self._h, int(b), float(t), _dp(E)))
         return E
+
+    def set_peierls(self, on=True):
+        """Propagate in the Peierls gauge (input key "peierls"); resets the
+        vector-potential integrators."""
+        self._check(self._L.edus_set_peierls(self._h, int(bool(on))))
+
+    def vector_potential(self, t, b=0):
+        """A(t) of solve b, advancing its integrator to t (Laser::VectorPotential)."""
+        A = np.empty(3)
+        self._check(self._L.edus_vector_potential(self._h, int(b), float(t), _dp(A)))
+        return A
 
     def upload_model_solve(self, b, H0k, xik):
         """A model of its own for solve b (FP64 form without HSEX)."""

@@ -191,6 +191,7 @@ class Config:
     printresolution: int = 1
     printresolution_pulse: int = 1  # 0 in the input means printresolution
     gradient_space: str = "R"  # "k": finite-difference gradient over k shells
+    peierls: bool = False  # propagation in the Peierls gauge (Functional_SourceTerm.hpp:15-50)
 
     @property
     def nsteps(self):
@@ -240,7 +241,8 @@ def parse_input(src, base_dir=None) -> Config:
                   edus.SOLVER_AB if d["solver"] == "AB" else edus.SOLVER_RK, int(d["order"]),
                   bool(d["coulomb"]), float(d["epsilon"]), r0, lasers,
                   bool(user.get("coulomb_fix_centres", False)), int(d["printresolution"]),
-                  int(d["printresolution_pulse"]) or int(d["printresolution"]), str(d["gradient_space"]))
+                  int(d["printresolution_pulse"]) or int(d["printresolution"]), str(d["gradient_space"]),
+                  bool(d["peierls"]))
 
 
 class Model:
@@ -422,4 +424,6 @@ class Model:
         for b in range(batch):
             s.set_lasers(cfg.lasers, b)
             s.set_state(self.rho0k, b)
+        if cfg.peierls:
+            s.set_peierls(True)
         return s

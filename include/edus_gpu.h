@@ -234,6 +234,23 @@ int edus_synchronize(edus_handle* h);
  * runs.  n = 0 restores the R-space gradient.  FP64 form. */
 int edus_set_kgradient(edus_handle* h, int n, const int* shift, const double* b, const double* w);
 
+/* Peierls gauge ("peierls": true; Functional_SourceTerm.hpp:15-50,
+ * Simulation.cpp:876-899): no gradient term, and the Hamiltonian of a stage at
+ * time t is H(R) = (H0(R) + E.xi(R) + Hee[rho(R) e^{-iA.R}](R)) e^{+iA.R},
+ * A(t) the vector potential of each solve's lasers integrated as
+ * Laser::VectorPotential does (Laser.cpp:136-151: one Simpson step from the
+ * previous requested time, from A = 0 at t = 0; every stage time and
+ * edus_vector_potential call is a request).  on = 1 resets the integrators;
+ * on = 0 returns to the length gauge.  FP64 form, one model for all solves,
+ * H0(R) and xi(R) on at most 4096 lattice vectors (tight-binding models). */
+int edus_set_peierls(edus_handle* h, int on);
+
+/* Vector potential of solve b advanced to time t (a request, as above), a.u.:
+ * Laser::VectorPotential summed over the solve's lasers (SetOfLaser,
+ * Laser.hpp:152-158; the reference's accumulator is shared by all lasers, so
+ * the two agree for one laser). */
+int edus_vector_potential(edus_handle* h, int b, double t, double* A);
+
 /* Observables of Simulation::do_onestep (Simulation.cpp:420-429).  Upload once
  * the eigenvectors U_k [Nk][nb][nb] (columns, SettingUp_EigenSystem) and/or the
  * velocity operator vel_k [3][Nk][nb][nb] (Simulation.cpp:523-576); either may

@@ -285,6 +285,7 @@ typedef struct {
     // propagate; it differs from the reference only on the N/2 planes.
     int hermitian_nyquist;
     int gradient_k;  // 1: gradient_space "k", the finite-difference gradient of kGradient.cpp
+    int peierls;     // 1: "peierls": true, propagation in the Peierls gauge
     int nlasers;
     oracle_laser lasers[8];
 } oracle_cfg;
@@ -319,6 +320,11 @@ struct Sim {
     double min_dist[3] = {100, 0, 0};
     double min_dist_norm = 100;
     std::vector<Laser> lasers;
+    // Peierls gauge: the vector potential integrator of Laser::VectorPotential
+    bool peierls = false;
+    double Avec[3] = {0., 0., 0.};
+    double Aprev = 0.;
+    std::vector<cd> auxR;
     // solver state
     int solver = 1, order = 4;
     double dt = 0, t = 0;
@@ -339,6 +345,36 @@ struct Sim {
             double e[3];
             l.field(time, e);
             for (int d = 0; d < 3; ++d) E[d] += e[d];
+        }
+    }
+
+    // Laser::VectorPotential (src/Laser/Laser.cpp:136-151): one Simpson step
+    // from the previous request, from A = 0 at t = 0.  The reference keeps A
+    // and the previous time in function statics shared by all lasers of
+    // SetOfLaser::VectorPotential (Laser.hpp:152-158); with one laser that is
+    // the integral of the total field, which is what this restates.
+    void vector_potential(double time, double out[3]) {
+        const double deltaT = time - Aprev;
+        if (deltaT >= 1.e-07) {
+            double E1[3], E2[3], E3[3];
+            efield(Aprev, E1);
+            efield(Aprev + deltaT / 2., E2);
+            efield(time, E3);
+            for (int d = 0; d < 3; ++d) Avec[d] -= deltaT / 6. * (E1[d] + 4. * E2[d] + E3[d]);
+            Aprev = time;
+        }
+        for (int d = 0; d < 3; ++d) out[d] = Avec[d];
+    }
+
+    // Simulation::Apply_Peierls_phase (Simulation.cpp:876-899): O(R) *= exp(i sign A(t).R)
+    void peierls_phase(cd* OR, double time, int sign) {
+        double At[3];
+        vector_potential(time, At);
+#pragma omp parallel for schedule(static)
+        for (int iR = 0; iR < Nk; ++iR) {
+            const double* R = &Rcart[3 * (size_t)iR];
+            const cd ph = std::exp(im * double(sign) * (At[0] * R[0] + At[1] * R[1] + At[2] * R[2]));
+            for (int p = 0; p < P; ++p) OR[(size_t)iR * P + p] *= ph;
         }
     }
 
@@ -445,6 +481,7 @@ Sim* build(const oracle_cfg* cfg) {
         for (int a = 0; a < 3; ++a) s.Rcart[3 * iR + a] = s.A[a][0] * c[0] + s.A[a][1] * c[1] + s.A[a][2] * c[2];
     }
     s.Rgrad = s.Rcart;
+    s.peierls = cfg->peierls != 0;
     if (cfg->gradient_k) build_kgradient(s);
     if (cfg->hermitian_nyquist) {
         for (int iR = 0; iR < Nk; ++iR) {
@@ -738,9 +775,11 @@ void source_term(Sim& s, cd* out_k, double time, const cd* in_k) {
     std::fill(s.outR.begin(), s.outR.end(), cd(0.));           // :16
     double E[3];
     s.efield(time, E);
-    // kGradient R branch: out(R) += 1 * i (R.E) in(R)  (kGradient_definitions.hpp:35-40)
+    // kGradient R branch: out(R) += 1 * i (R.E) in(R)  (kGradient_definitions.hpp:35-40);
+    // no gradient term in the Peierls gauge (Functional_SourceTerm.hpp:20)
+    const bool grad = !s.peierls;
 #pragma omp parallel for schedule(static)
-    for (int iR = 0; iR < (s.gw.empty() ? s.Nk : 0); ++iR) {
+    for (int iR = 0; iR < (grad && s.gw.empty() ? s.Nk : 0); ++iR) {
         const double* Rc = &s.Rgrad[3 * (size_t)iR];
         double dot = Rc[0] * E[0] + Rc[1] * E[1] + Rc[2] * E[2];
         for (int p = 0; p < P; ++p) s.outR[(size_t)iR * P + p] += (1. + 0. * im) * im * dot * s.inR[(size_t)iR * P + p];
@@ -751,17 +790,26 @@ void source_term(Sim& s, cd* out_k, double time, const cd* in_k) {
         s.HR[i] = 0.;
         s.HR[i] += s.H0R[i] + E[0] * s.rR[0][i] + E[1] * s.rR[1][i] + E[2] * s.rR[2][i];
     }
+    // Peierls gauge: the self-energy sees rho(R) e^{-iA.R} (Functional_SourceTerm.hpp:31-38)
+    const cd* DM = s.inR.data();
+    if (s.peierls) {
+        s.auxR = s.inR;
+        s.peierls_phase(s.auxR.data(), time, -1);
+        DM = s.auxR.data();
+    }
     // Coulomb::EffectiveHamiltonian (Coulomb.cpp:134-180)
     if (s.coulomb) {
         const size_t o = (size_t)s.origin * P;
         for (int n = 0; n < nb; ++n)
             for (int m = 0; m < nb; ++m)
-                s.HR[o + n * nb + n] += s.Hartree[n * nb + m] * (s.inR[o + m * nb + m] - s.DM0R[o + m * nb + m]);
+                s.HR[o + n * nb + n] += s.Hartree[n * nb + m] * (DM[o + m * nb + m] - s.DM0R[o + m * nb + m]);
 #pragma omp parallel for schedule(static)
-        for (long i = 0; i < (long)S; ++i) s.HR[i] -= s.W[i] * (s.inR[i] - s.DM0R[i]);
+        for (long i = 0; i < (long)S; ++i) s.HR[i] -= s.W[i] * (DM[i] - s.DM0R[i]);
     }
+    // H(R) *= e^{+iA.R} (Functional_SourceTerm.hpp:41-44)
+    if (s.peierls) s.peierls_phase(s.HR.data(), time, +1);
     s.fft.run(s.outR.data(), out_k, +1);                       // :49 Output.go_to_k
-    if (!s.gw.empty()) {
+    if (grad && !s.gw.empty()) {
         // kGradient k branch (kGradient_definitions.hpp:18-30): out(k) += sum w (b.E) in(k + b)
 #pragma omp parallel for schedule(static)
         for (int ik = 0; ik < s.Nk; ++ik) {
@@ -915,11 +963,23 @@ void oracle_step(void* h, int n) {
 int oracle_observables(void* h, double* pop_bloch, double* pop_wannier, double* vel) {
     Sim& s = *static_cast<Sim*>(h);
     const int nb = s.nb, P = s.P;
+    // Peierls gauge: the observables see rho(R) e^{-iA.R} at CurrentTime
+    // (Simulation.cpp:447-449, 593-595)
+    const cd* rho = s.rho.data();
+    std::vector<cd> shifted;
+    if (s.peierls) {
+        std::vector<cd> R(s.S());
+        shifted.resize(s.S());
+        s.fft.run(s.rho.data(), R.data(), -1);
+        s.peierls_phase(R.data(), s.t, -1);
+        s.fft.run(R.data(), shifted.data(), +1);
+        rho = shifted.data();
+    }
     std::vector<double> pb(nb, 0.), pw(nb, 0.);
     std::vector<cd> tmp(P), rb(P), Ud(P);
     for (int ik = 0; ik < s.Nk; ++ik) {
         const cd* Uk = &s.U[(size_t)ik * P];
-        const cd* r = &s.rho[(size_t)ik * P];
+        const cd* r = &rho[(size_t)ik * P];
         for (int i = 0; i < nb; ++i)
             for (int j = 0; j < nb; ++j) Ud[i * nb + j] = std::conj(Uk[j * nb + i]);
         matmul(nb, Ud.data(), r, tmp.data(), 1., 0.);
@@ -943,7 +1003,7 @@ int oracle_observables(void* h, double* pop_bloch, double* pop_wannier, double* 
         cd v = 0.;
         for (int ik = 0; ik < s.Nk; ++ik) {
             const cd* a = &s.vel[d][(size_t)ik * P];
-            const cd* r = &s.rho[(size_t)ik * P];
+            const cd* r = &rho[(size_t)ik * P];
             for (int n = 0; n < nb; ++n)
                 for (int k = 0; k < nb; ++k) v += a[n * nb + k] * r[k * nb + n];
         }
@@ -955,6 +1015,9 @@ int oracle_observables(void* h, double* pop_bloch, double* pop_wannier, double* 
 }
 
 double oracle_struve0(double x) { return oracle::struve0(x); }
+
+// SetOfLaser::VectorPotential at t (advances the integrator, as every request does)
+void oracle_vector_potential(void* h, double t, double* out) { static_cast<Sim*>(h)->vector_potential(t, out); }
 
 // standalone FFT of `howmany` interleaved planes on an N0xN1xN2 grid
 void oracle_fft(const int* dims, int howmany, const double* in, double* out, int sign) {

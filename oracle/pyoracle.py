@@ -114,6 +114,7 @@ class SimConfig:
     hermitian_nyquist: bool = False  # test switch: the packed forms' Hermitian generator
     printresolution: int = 1
     printresolution_pulse: int = 1
+    peierls: bool = False
 
     @property
     def nsteps(self) -> int:
@@ -177,7 +178,7 @@ def load_input(src, base_dir: str | None = None) -> SimConfig:
         coulomb=bool(d["coulomb"]), epsilon=float(d["epsilon"]), r0=tuple(r0),
         gradient_space=str(d["gradient_space"]), lasers=las,
         coulomb_fix_centres=bool(d.get("coulomb_fix_centres", False)),
-        printresolution=pr, printresolution_pulse=prp,
+        printresolution=pr, printresolution_pulse=prp, peierls=bool(d["peierls"]),
     )
 
 
@@ -195,6 +196,7 @@ class _Cfg(ctypes.Structure):
                 ("epsilon", ctypes.c_double), ("r0_au", ctypes.c_double * 3),
                 ("nr0", ctypes.c_int), ("coulomb_fix_centres", ctypes.c_int),
                 ("hermitian_nyquist", ctypes.c_int), ("gradient_k", ctypes.c_int),
+                ("peierls", ctypes.c_int),
                 ("nlasers", ctypes.c_int), ("lasers", _Laser * 8)]
 
 
@@ -233,6 +235,7 @@ def lib():
         L.oracle_rhs.argtypes = [ctypes.c_void_p, ctypes.c_double, dp, dp]
         L.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oracle_observables.argtypes = [ctypes.c_void_p, dp, dp, dp]
+        L.oracle_vector_potential.argtypes = [ctypes.c_void_p, ctypes.c_double, dp]
         L.oracle_struve0.restype = ctypes.c_double
         L.oracle_struve0.argtypes = [ctypes.c_double]
         L.oracle_fft.argtypes = [P(ctypes.c_int), ctypes.c_int, dp, dp, ctypes.c_int]
@@ -262,6 +265,7 @@ def make_cfg(cfg: SimConfig) -> _Cfg:
     c.coulomb_fix_centres = int(cfg.coulomb_fix_centres)
     c.hermitian_nyquist = int(cfg.hermitian_nyquist)
     c.gradient_k = 1 if cfg.gradient_space == "k" else 0
+    c.peierls = int(cfg.peierls)
     if len(cfg.lasers) > 8:
         raise ValueError("at most 8 lasers")
     c.nlasers = len(cfg.lasers)
@@ -359,6 +363,12 @@ class Oracle:
 
     def step(self, n: int = 1):
         lib().oracle_step(self.h, int(n))
+
+    def vector_potential(self, t: float) -> np.ndarray:
+        """A(t), advancing the integrator to t (Laser::VectorPotential)."""
+        A = np.zeros(3)
+        lib().oracle_vector_potential(self.h, float(t), _dp(A))
+        return A
 
     def observables(self):
         """Population (Bloch, Wannier) and velocity rows as the reference prints them."""

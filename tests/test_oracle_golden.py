@@ -313,3 +313,50 @@ def test_k_gradient_stencil_model_equals_property(pkg, tmp_path):
         want = np.diag([1.0 if n > 1 else 0.0 for n in grid])
         assert np.abs(M - want).max() < 1e-8
         assert np.abs(np.einsum("i,ia->a", w, b)).max() < 1e-8  # symmetric shells
+
+
+def _peierls_oracle(po, pkg, tmp_path, name, coulomb, envelope="sin2"):
+    uc, Rs, H, r = pkg.workloads.random_model(3, 7)
+    seed = os.path.join(str(tmp_path), name)
+    pkg.workloads.write_tb(seed + "_tb.dat", uc, Rs, H, r)
+    las = ([pkg.workloads.sin2_laser(2.0, 5e12, 3, pol=(1.0, 0.4, 0.2))] if envelope == "sin2" else
+           [pkg.workloads.gaussian_laser(1.5, 0.5, 0.02, 0.3, pol=(0.6, 1.0, 0.0))])
+    inp = pkg.workloads._input(seed, (6, 8, 1), 1, 0.01, 10, "RK", las, coulomb=coulomb, epsilon=2.0, r0_A=10.0)
+    inp["peierls"] = True
+    cfg = po.load_input(inp)
+    inp2 = dict(inp)
+    inp2["peierls"] = False
+    return po.Oracle(cfg), po.Oracle(po.load_input(inp2))
+
+
+def test_peierls_vector_potential_integrator(po, pkg, tmp_path):
+    """Laser::VectorPotential (Laser.cpp:136-151): one Simpson step from the
+    previous request, none below 1e-7, from A = 0 at t = 0; close to -int E dt."""
+    o, _ = _peierls_oracle(po, pkg, tmp_path, "pvec", False, envelope="gauss")
+    A = np.zeros(3)
+    prev = 0.0
+    ts = np.concatenate([np.linspace(0.0, 400.0, 401), [400.0, 400.0 + 5e-8, 401.0]])
+    for t in ts:
+        got = o.vector_potential(t)
+        dT = t - prev
+        if dT >= 1e-7:
+            A = A - dT / 6.0 * (o.efield(prev) + 4.0 * o.efield(prev + dT / 2.0) + o.efield(t))
+            prev = t
+        assert np.array_equal(got, A)
+    # the rule integrates the field: against a fine trapezoid sum of -E
+    fine = np.linspace(0.0, 401.0, 40101)
+    Ef = np.array([o.efield(t) for t in fine])
+    ref = -np.trapezoid(Ef, fine, axis=0)
+    assert np.abs(A - ref).max() < 1e-6 * max(np.abs(ref).max(), 1e-3)
+
+
+@pytest.mark.parametrize("coulomb", [False, True])
+def test_peierls_without_field_is_the_length_gauge(po, pkg, tmp_path, coulomb):
+    """Before a sin^2 pulse E = 0 and A = 0: the two gauges give the same source term."""
+    op, ol = _peierls_oracle(po, pkg, tmp_path, f"pzero{int(coulomb)}", coulomb)
+    rng = np.random.default_rng(3)
+    rho = op.get("rho") + 0.1 * (rng.normal(size=op.get("rho").shape) + 1j * rng.normal(size=op.get("rho").shape))
+    t = 0.5 * op.cfg.lasers[0].t0
+    assert np.array_equal(op.efield(t), np.zeros(3))
+    a, b = op.rhs(t, rho), ol.rhs(t, rho)
+    assert np.abs(a - b).max() <= 1e-15 * np.abs(b).max()
