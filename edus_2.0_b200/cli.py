@@ -21,17 +21,39 @@ each step whose time t has int(round(t/dt)) % printresolution_pulse == 0
     Velocity.txt            re, im of the x, y, z velocity
 
 The observables are computed on the GPU (edus_observables; in the Peierls gauge
-of the state rho(R) e^{-iA.R}, Simulation.cpp:447-449, 593-595).  Differences from
-the reference: the vector potential integrates the total field of all lasers
-(the reference's accumulator is a function-static shared by every laser, which
-only agrees for a single laser); output.h5 is not written.
+of the state rho(R) e^{-iA.R}, Simulation.cpp:447-449, 593-595).
+
+output.h5 (Simulation.cpp:202-233, 384-416; GlobalFunctions.cpp:22-66) is written
+by the package's own HDF5 writer (h5.py) in the reference's layout:
+
+    json/...                         the input (tb_file, coulomb, grid, filledbands,
+                                     dt, printresolution, initialtime, finaltime,
+                                     num_bands, num_kpoints, solver, laser<i>/...,
+                                     kpoints, A, B) as dump_json_in_h5 writes it
+    fullH, DensityMatrix_k,          per printed step <it> (0, 1, ...):
+    DensityMatrix_k_bloch,           <node>/<it>/0/local, the [k][n][m] complex
+    SelfEnergy                       matrix as 2 Nk nb^2 doubles, for the
+                                     quantities that "toprint" selects
+    time_au/<it>                     CurrentTime of print <it>
+
+A step is printed there when int(round(t/dt)) % r == 0 with r = the pulse print
+resolution inside any laser's window and printresolution outside it
+(PrintObservables(t, true), Simulation.cpp:236-257).  The Gaussian-envelope
+lasers (an extension) count t0 +- 3 fwhm as their window.
+
+Differences from the reference: the vector potential integrates the total field
+of all lasers (the reference's accumulator is a function-static shared by every
+laser, which only agrees for a single laser).
 """
 from __future__ import annotations
 
 import argparse
 import importlib.util
+import json
 import os
 import sys
+
+import numpy as np
 
 
 def _package():
@@ -46,25 +68,123 @@ def _package():
     return mod
 
 
+TOPRINT = {"DMk_wannier": "DensityMatrix_k", "DMk_bloch": "DensityMatrix_k_bloch", "fullH": "fullH",
+           "SelfEnergy": "SelfEnergy"}
+
+
+def _raw_input(input_path: str, pkg) -> dict:
+    with open(input_path) as f:
+        user = json.load(f)
+    d = dict(pkg.model.SCHEMA_DEFAULTS)
+    d.update({k: v for k, v in user.items() if k != "lasers"})
+    d["lasers"] = [dict(pkg.model.LASER_DEFAULTS, **L) for L in user.get("lasers", [])]
+    d["toprint"] = dict({k: "false" for k in TOPRINT}, **user.get("toprint", {}))
+    return d
+
+
+def _h5_json(h5, raw: dict, m) -> None:
+    """dump_json_in_h5 (GlobalFunctions.cpp:22-66); "polarization" of each laser
+    receives its "cycles", as the reference writes it."""
+    j = h5.group("json")
+    j.write("tb_file", str(raw["tb_file"]))
+    j.write("coulomb", int(bool(raw["coulomb"])))
+    j.write("grid", np.array([int(x) for x in raw["grid"]], dtype=np.int32))
+    j.write("filledbands", int(raw["filledbands"]))
+    j.write("dt", float(raw["dt"]))
+    j.write("printresolution", int(raw["printresolution"]))
+    j.write("initialtime", float(raw["initialtime"]))
+    j.write("finaltime", float(raw["finaltime"]))
+    j.write("num_bands", int(m.nb))
+    j.write("num_kpoints", int(m.Nk))
+    j.write("solver", str(raw["solver"]))
+    for i, L in enumerate(raw["lasers"]):
+        g = j.group(f"laser{i}")
+        g.write("intensity", float(L["intensity"]))
+        g.write("frequency", float(L["frequency"]))
+        g.write("wavelength", float(L["wavelength"]))
+        g.write("cycles", int(L["cycles"]))
+        g.write("polarization", int(L["cycles"]))
+    # bare k (crystal coordinates, ix / N) and the bases (Simulation.cpp:207-216)
+    N = m.grid
+    idx = np.indices(N).reshape(3, -1).T
+    j.write("kpoints", (idx / np.array(N, dtype=float)).reshape(-1))
+    j.write("A", m.A.reshape(-1))
+    j.write("B", (2.0 * np.pi * np.linalg.inv(m.A).T).reshape(-1))
+
+
+def _in_pulse(t: float, lasers) -> bool:
+    pkg = _package()
+    for L in lasers:
+        if L.envelope == pkg.edus.ENVELOPE_SIN2:
+            t1 = L.t0 + L.cycles * 2.0 * np.pi / L.omega
+            if L.t0 + 1e-7 < t < t1 + 1e-7:
+                return True
+        elif abs(t - L.t0) < 3.0 * L.fwhm:
+            return True
+    return False
+
+
+def _self_energy_k(m, rho_k):
+    """Coulomb::EffectiveHamiltonian with H erased (Coulomb.cpp:134-180), to k."""
+    pkg = _package()
+    rR = pkg.model.fft_k_to_R(rho_k, m.grid)
+    sig = -m.W * (rR - m.DM0R)
+    d = np.diagonal(rR[0]) - np.diagonal(m.DM0R[0])
+    sig[0][np.diag_indices(m.nb)] += m.hartree @ d
+    return pkg.model.fft_R_to_k(sig, m.grid)
+
+
 def run(input_path: str, outdir: str, device: int = 0) -> int:
-    """Propagate and write the text outputs; returns the number of steps."""
+    """Propagate and write the text outputs and output.h5; returns the number of steps."""
     pkg = _package()
     cfg = pkg.model.parse_input(input_path)
+    raw = _raw_input(input_path, pkg)
     m = pkg.model.Model(cfg)
     s = m.solver(device=device)
     s.upload_observables(U=m.U, vel=m.velocity())
     os.makedirs(outdir, exist_ok=True)
     names = ("Time", "Laser", "Laser_A", "Population", "Population_wannier", "Velocity")
     files = {n: open(os.path.join(outdir, n + ".txt"), "w") for n in names}
+    h5 = pkg.h5.H5Tree()
+    _h5_json(h5, raw, m)
+    for node in ("fullH", "DensityMatrix_k", "DensityMatrix_k_bloch", "SelfEnergy", "time_au"):
+        h5.group(node)
+    wanted = [k for k in TOPRINT if str(raw["toprint"].get(k, "false")).lower() == "true"]
+    if "SelfEnergy" in wanted and not cfg.coulomb:
+        wanted.remove("SelfEnergy")  # no self-energy without HSEX: nothing to write
     dt = cfg.dt
     pr = max(1, int(cfg.printresolution_pulse))
+    pr_out = max(1, int(cfg.printresolution))
     nsteps = cfg.nsteps
     A = [0.0, 0.0, 0.0]
     t_prev = 0.0
+    it_h5 = 0
+
+    def h5_due(t):
+        r = pr if _in_pulse(t, cfg.lasers) else pr_out
+        return int(round(t / dt)) % r == 0
+
     try:
         t = s.time  # the library's CurrentTime: accumulated by += dt, as DESolver does
         it = 0
         while it < nsteps:
+            if h5_due(t):
+                # Simulation::do_onestep (Simulation.cpp:384-416)
+                node = str(it_h5)
+                rho = s.get_state() if wanted else None
+                for key in wanted:
+                    if key == "DMk_wannier":
+                        mat = rho
+                    elif key == "DMk_bloch":
+                        mat = np.einsum("kji,kjl,klm->kim", m.U.conj(), rho, m.U)
+                    elif key == "fullH":
+                        E = s.efield(t)
+                        mat = m.H0k + E[0] * m.xik[0] + E[1] * m.xik[1] + E[2] * m.xik[2]
+                    else:
+                        mat = _self_energy_k(m, rho)
+                    h5[TOPRINT[key]].group(node).group("0").write("local", np.ascontiguousarray(mat))
+                h5["time_au"].write(node, float(t))
+                it_h5 += 1
             if int(round(t / dt)) % pr == 0:
                 E = s.efield(t)
                 if cfg.peierls:
@@ -85,7 +205,7 @@ def run(input_path: str, outdir: str, device: int = 0) -> int:
             # step to the next printed time (or the end) in one call
             n = 1
             tn = t + dt
-            while it + n < nsteps and int(round(tn / dt)) % pr != 0:
+            while it + n < nsteps and int(round(tn / dt)) % pr != 0 and not h5_due(tn):
                 n += 1
                 tn += dt
             s.step(n)
@@ -97,6 +217,7 @@ def run(input_path: str, outdir: str, device: int = 0) -> int:
         for f in files.values():
             f.close()
     s.synchronize()
+    h5.save(os.path.join(outdir, "output.h5"))
     return nsteps
 
 

@@ -68,3 +68,63 @@ def test_observables_match_host(pkg, tmp_path):
     assert np.abs(pw - ref_w).max() < 1e-13
     assert np.abs(v - ref_v).max() < 1e-13 * max(1.0, np.abs(ref_v).max())
     assert np.abs(ref_v).max() > 1e-8  # a real signal
+
+
+def test_cli_output_h5(pkg, po, tmp_path):
+    """output.h5 in the reference's layout: the input under json/, and per step
+    printed there the density matrix (Wannier and Bloch gauge), H0 + E.xi and the
+    self-energy at the FP64 bar against the oracle, with time_au/<it>."""
+    inp = model_input(pkg, tmp_path, "h5cli", (6, 6, 1), nb=3, coulomb=True, dt=0.01, envelope="gauss")
+    inp["printresolution"] = 3
+    inp["printresolution_pulse"] = 2
+    inp["toprint"] = {"DMk_wannier": "true", "DMk_bloch": "true", "fullH": "true", "SelfEnergy": "true"}
+    path = os.path.join(str(tmp_path), "h5cli.json")
+    with open(path, "w") as f:
+        json.dump(inp, f)
+    out = os.path.join(str(tmp_path), "Out")
+    from edus_b200 import cli
+
+    n = cli.run(path, out)
+    got = pkg.h5.read_h5(os.path.join(out, "output.h5"))
+    j = got["json"]
+    assert bytes(j["tb_file"]).decode() == inp["tb_file"]
+    assert j["grid"].tolist() == [6, 6, 1] and j["num_bands"].tolist() == [3] and j["num_kpoints"].tolist() == [36]
+    assert j["coulomb"].tolist() == [1] and bytes(j["solver"]).decode() == "RK"
+    assert np.allclose(j["kpoints"].reshape(36, 3)[1], [0.0, 1.0 / 6.0, 0.0])
+    assert j["laser0"]["polarization"].tolist() == j["laser0"]["cycles"].tolist()
+    cfg = po.load_input(path)
+    o = po.Oracle(cfg)
+    Nk, nb = 36, 3
+    U = o.get("U")
+    Um = pkg.model.Model(pkg.model.parse_input(path)).U
+    W, DM0R, hart = o.get("W"), o.get("DM0R"), o.hartree()
+    xi = [o.get("xk"), o.get("yk"), o.get("zk")]
+    times = got["time_au"]
+    assert len(times) >= 3
+    printed = {round(float(times[str(i)][0]) / cfg.dt): str(i) for i in range(len(times))}
+    for step in range(n):
+        if step in printed:
+            it = printed[step]
+            t = float(times[it][0])
+            rho = o.get("rho")
+            dm = got["DensityMatrix_k"][it]["0"]["local"].view(np.complex128).reshape(Nk, nb, nb)
+            assert np.abs(dm - rho).max() < 1e-10 * np.abs(rho).max(), step
+            # Bloch gauge with the model's eigenvectors (their phases are a choice: the
+            # oracle's differ, so against it only the phase-free parts are compared)
+            dmb = got["DensityMatrix_k_bloch"][it]["0"]["local"].view(np.complex128).reshape(Nk, nb, nb)
+            rb = np.einsum("kji,kjl,klm->kim", Um.conj(), rho, Um)
+            assert np.abs(dmb - rb).max() < 1e-10 * np.abs(rb).max(), step
+            ro = np.einsum("kji,kjl,klm->kim", U.conj(), rho, U)
+            assert np.abs(np.abs(dmb) - np.abs(ro)).max() < 1e-9 * np.abs(ro).max(), step
+            E = o.efield(t)
+            H = got["fullH"][it]["0"]["local"].view(np.complex128).reshape(Nk, nb, nb)
+            Href = o.get("H0k") + E[0] * xi[0] + E[1] * xi[1] + E[2] * xi[2]
+            assert np.abs(H - Href).max() < 1e-13 * np.abs(Href).max(), step
+            rR = np.fft.fftn(rho.reshape(6, 6, 1, nb, nb), axes=(0, 1, 2)).reshape(Nk, nb, nb) / Nk
+            sig = -W * (rR - DM0R)
+            sig[0][np.diag_indices(nb)] += hart @ (np.diagonal(rR[0]) - np.diagonal(DM0R[0]))
+            sref = np.fft.ifftn(sig.reshape(6, 6, 1, nb, nb), axes=(0, 1, 2)).reshape(Nk, nb, nb) * Nk
+            S = got["SelfEnergy"][it]["0"]["local"].view(np.complex128).reshape(Nk, nb, nb)
+            # at the first steps rho = rho0 and the self-energy is rounding: bound by |W| |rho|
+            assert np.abs(S - sref).max() < 1e-10 * np.abs(W).max() * np.abs(rho).max(), step
+        o.step(1)
