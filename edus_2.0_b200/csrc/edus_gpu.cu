@@ -502,8 +502,10 @@ PFN_cuTensorMapEncodeTiled tensor_map_encoder() {
 }
 
 // The [nbatch][P][Nk] complex array at `base` as the 4-D tensor
-// {2 Nk, nb, nb, nbatch} of doubles, box {2 TK, nb, nb, 1} (padded = false)
-// or {2 TK, nbp + 1, nbp, 1} (padded = true: the copy zero-fills the margin).
+// {2 Nk, nb, nb, nbatch} of doubles, box {2 TKU, nb, nb, 1} (padded = false:
+// the update operands, 4 k points) or {2 TK, W, nb, 1} (padded = true: the
+// product operands, 2 k points, rows of odd length W; the copy zero-fills a
+// column beyond nb).
 const CUtensorMap* operand_map(edus_handle* h, const void* base, int nbatch, bool padded) {
     const auto key = std::make_pair(base, 2 * nbatch + (padded ? 1 : 0));
     auto it = h->tmaps.find(key);
@@ -514,10 +516,10 @@ const CUtensorMap* operand_map(edus_handle* h, const void* base, int nbatch, boo
     const cuuint64_t nb = (cuuint64_t)h->nb, Nk = (cuuint64_t)h->Nk;
     const cuuint64_t dims[4] = {2 * Nk, nb, nb, (cuuint64_t)nbatch};
     const cuuint64_t strides[3] = {Nk * 16, nb * Nk * 16, nb * nb * Nk * 16};
-    cuuint32_t box[4] = {(cuuint32_t)(2 * g.TK), (cuuint32_t)nb, (cuuint32_t)nb, 1};
+    cuuint32_t box[4] = {(cuuint32_t)(2 * g.TKU), (cuuint32_t)nb, (cuuint32_t)nb, 1};
     if (padded) {
+        box[0] = (cuuint32_t)(2 * g.TK);
         box[1] = (cuuint32_t)g.W;
-        box[2] = (cuuint32_t)g.nbp;
     }
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     CUtensorMap m;
@@ -531,7 +533,7 @@ const CUtensorMap* operand_map(edus_handle* h, const void* base, int nbatch, boo
 template <int MODE>
 int launch_ws(edus_handle* h, const StageArgs& a, int nbatch) {
     const WsGeom g = ws_geometry(h->nb);
-    const int ntiles = ((h->Nk + g.TK - 1) / g.TK) * nbatch;
+    const int ntiles = ((h->Nk + g.TKU - 1) / g.TKU) * nbatch;  // update tiles
     const int grid = std::min(ntiles, h->ws_grid);
     OperandMaps maps;
     const void* src[5] = {a.Hee, a.rho, a.G, a.y ? (const void*)a.y : (const void*)a.G,
@@ -541,10 +543,12 @@ int launch_ws(edus_handle* h, const StageArgs& a, int nbatch) {
         if (!m) return fail(h, EDUS_ERR_CUDA, "cuTensorMapEncodeTiled failed for a commutator operand");
         maps.m[i] = *m;
     }
-    if (g.tiles == 3)
-        commutator_ws_kernel<MODE, 3><<<grid, g.threads, g.smem, h->stream>>>(a, nbatch, maps, h->flag);
+    if (g.tiles == 2)
+        commutator_ws_kernel<MODE, 2, 4><<<grid, g.threads, g.smem, h->stream>>>(a, nbatch, maps, h->flag);
+    else if (g.SM == 3)
+        commutator_ws_kernel<MODE, 3, 3><<<grid, g.threads, g.smem, h->stream>>>(a, nbatch, maps, h->flag);
     else
-        commutator_ws_kernel<MODE, 2><<<grid, g.threads, g.smem, h->stream>>>(a, nbatch, maps, h->flag);
+        commutator_ws_kernel<MODE, 3, 2><<<grid, g.threads, g.smem, h->stream>>>(a, nbatch, maps, h->flag);
     return EDUS_OK;
 }
 
@@ -1158,16 +1162,20 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
         const WsGeom wg = ws_geometry(h->nb);
         if ((int)wg.smem <= dev_smem) {
 #define SETW(M)                                                                                           \
-    if ((rc = set_smem(h, commutator_ws_kernel<M, 3>, (int)wg.smem))) return bail(rc);       \
-    if ((rc = set_smem(h, commutator_ws_kernel<M, 2>, (int)wg.smem))) return bail(rc);
+    if ((rc = set_smem(h, commutator_ws_kernel<M, 3, 3>, (int)wg.smem))) return bail(rc);    \
+    if ((rc = set_smem(h, commutator_ws_kernel<M, 3, 2>, (int)wg.smem))) return bail(rc);    \
+    if ((rc = set_smem(h, commutator_ws_kernel<M, 2, 4>, (int)wg.smem))) return bail(rc);
             SETW(MODE_RHS) SETW(MODE_RK1) SETW(MODE_RK2) SETW(MODE_RK3) SETW(MODE_RK4) SETW(MODE_AB)
 #undef SETW
             int per_sm = 0;
-            if (wg.tiles == 3)
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commutator_ws_kernel<MODE_RK2, 3>,
+            if (wg.tiles == 2)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commutator_ws_kernel<MODE_RK2, 2, 4>,
+                                                              wg.threads, wg.smem);
+            else if (wg.SM == 3)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commutator_ws_kernel<MODE_RK2, 3, 3>,
                                                               wg.threads, wg.smem);
             else
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commutator_ws_kernel<MODE_RK2, 2>,
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, commutator_ws_kernel<MODE_RK2, 3, 2>,
                                                               wg.threads, wg.smem);
             int nsm = 0;
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, d.device);

@@ -233,7 +233,10 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     const double* rp1 = rpos + pl.ax[1].rposoff;
     const double* rp2 = rpos + pl.ax[2].rposoff;
     for (int w = blockIdx.x; w < nplanes; w += gridDim.x) {
-        const int b = w / P, p = w - (w / P) * P;
+        // the solves of one band-pair plane run side by side: rho0 and W, which
+        // they share, come from HBM once and from L2 for the others
+        const int nbat = nplanes / P;
+        const int p = w / nbat, b = w - (w / nbat) * nbat;
         if (ptab) {
             // Peierls gauge: no gradient term, two transforms (one without
             // HSEX); H = (H0 + E.xi + Hee[rho e^{-iA.R}]) e^{iA.R}

@@ -114,8 +114,10 @@ def test_steps_parity(pkg, po, tmp_path, solver, order, coulomb):
 
 
 # the fused HSEX commutator for 12 <= nb <= 24: 8x8 tiles in 2x2 (nb 13) and 3x3
-# (nb 19, 24) blocks; an odd k count (35) leaves the last tile one k point short
-@pytest.mark.parametrize("nb,grid", [(13, (8, 9, 1)), (19, (7, 5, 1)), (24, (6, 4, 1))])
+# (nb 17, 19, 24) blocks; k counts 72, 35, 25 and 30 (0, 3, 1 and 2 mod 4) end the
+# last update tile of 4 k points full, one short, with its second product tile
+# wholly past the grid, and two short
+@pytest.mark.parametrize("nb,grid", [(13, (8, 9, 1)), (19, (7, 5, 1)), (24, (5, 5, 1)), (17, (5, 6, 1))])
 @pytest.mark.parametrize("solver,order", [("RK", 4), ("AB", 4)])
 def test_steps_parity_mma(pkg, po, tmp_path, solver, order, nb, grid):
     inp = model_input(pkg, tmp_path, f"stm_{solver}{order}_{nb}", grid, nb=nb, coulomb=True, solver=solver,
