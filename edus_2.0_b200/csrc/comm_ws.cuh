@@ -37,7 +37,9 @@
 // each lane loads both k points of its element in the order set by the parity
 // of its row.  Fragment rows and columns beyond nb (the 8x8 tiles cover nb
 // rounded up to 8) are not loaded: they read as zero.  Update operands are
-// dense [P][4], C is staged [P][2] per product tile.  A product tile past the last k point (Nk = 1 mod 4) is copied
+// dense [P][4]; C is staged per product tile as [k point][row][CW] with CW odd
+// and the k-point stride R = 4 (mod 8) 16-byte units, which keeps both the
+// fragment-layout stores and the update warps' reads free of bank conflicts.  A product tile past the last k point (Nk = 1 mod 4) is copied
 // as zeros and its results are not written.
 //
 // Per k step and k point the products are 8 m8n8k4 (H rho - rho H from real
@@ -54,10 +56,11 @@ namespace edus {
 
 struct WsGeom {
     int TK, TKU, nbp, tiles, W, NM, NE, warps, threads, jobs, SM;
+    int CW, CR;           // staged C: row length (odd) and k-point stride (4 mod 8), complex units
     size_t mop_bytes;     // one product operand [nb][W][TK] complex, a 128-byte multiple
     size_t hh_off;        // Hartree shifts [nb] after H and rho
     size_t mstage_bytes;  // H, rho, hh
-    size_t arr_bytes;     // one staged C [P][TK], a 128-byte multiple
+    size_t arr_bytes;     // one staged C [TK][nb][CW] (k-point stride CR), a 128-byte multiple
     size_t uarr_bytes;    // one update operand [P][TKU], a 128-byte multiple
     size_t off_e, off_c, off_bar, smem;
 };
@@ -81,7 +84,9 @@ __host__ __device__ inline WsGeom ws_geometry(int nb) {
     g.mop_bytes = ((size_t)nb * g.W * g.TK * 16 + 127) & ~(size_t)127;
     g.hh_off = 2 * g.mop_bytes;
     g.mstage_bytes = g.hh_off + (((size_t)nb * 16 + 127) & ~(size_t)127);
-    g.arr_bytes = ((size_t)nb * nb * g.TK * 16 + 127) & ~(size_t)127;
+    g.CW = (nb & 1) ? nb : nb + 1;
+    g.CR = nb * g.CW + ((4 - nb * g.CW) & 7);
+    g.arr_bytes = ((size_t)g.TK * g.CR * 16 + 127) & ~(size_t)127;
     g.uarr_bytes = ((size_t)nb * nb * g.TKU * 16 + 127) & ~(size_t)127;
     for (g.SM = g.tiles == 2 ? 4 : 3;; --g.SM) {
         g.off_e = g.SM * g.mstage_bytes;
@@ -281,7 +286,7 @@ __global__ void __launch_bounds__(32 * (2 + 2 * (TILES == 3 ? 8 : 4)), 1)
                     for (int kk = 0; kk < 2; ++kk) {
                         double2 c = make_double2(qq ? c1[kk][0] : c0[kk][0], qq ? c1[kk][1] : c0[kk][1]);
                         c = cadd(c, cmul(dh, Rm[(row * W + col) * TK + kk]));
-                        Cs[(row * nb + col) * TK + kk] = c;
+                        Cs[kk * g.CR + row * g.CW + col] = c;
                     }
                 }
             }
@@ -297,6 +302,7 @@ __global__ void __launch_bounds__(32 * (2 + 2 * (TILES == 3 ? 8 : 4)), 1)
     // ---- update warps: half h of update tile j, element (p, kk) at k0 + 2 h + kk
     const int ew = warp - 2 - NM;
     const double2 zero = make_double2(0.0, 0.0);
+    const FastDiv fd_nb = {((1ull << 40) + (unsigned long long)nb - 1ull) / (unsigned long long)nb, nb};
     for (int j = 0; j < nit; ++j) {
         const unsigned par = (unsigned)(j & 1);
         const int u = blockIdx.x + j * gridDim.x;
@@ -311,13 +317,14 @@ __global__ void __launch_bounds__(32 * (2 + 2 * (TILES == 3 ? 8 : 4)), 1)
                 if (lane == 0) atomicOr(status, 1);
                 return;
             }
-            const double2* Cs = (const double2*)(base + g.off_c + h * g.arr_bytes);  // [P][TK]
+            const double2* Cs = (const double2*)(base + g.off_c + h * g.arr_bytes);  // [TK][nb][CW]
             for (int idx = ew * 32 + lane; idx < P * TK; idx += NE * 32) {
-                const int p = idx >> 1, kq = 2 * h + (idx & 1);
+                const int p = idx >> 1, kk = idx & 1, kq = 2 * h + kk;
                 if (k0 + kq >= Nk) continue;
                 const long long e = boff + (long long)p * Nk + k0 + kq;
                 const int eu = p * TKU + kq;  // in the update operands [P][TKU]
-                const double2 c = Cs[idx];
+                const int row = fdiv(p, fd_nb), col = p - row * nb;
+                const double2 c = Cs[kk * g.CR + row * g.CW + col];
                 const double2 gg = Gs[eu];
                 const double2 f = make_double2(gg.x + c.y, gg.y - c.x);  // f = G - i C
                 double2 yv = zero, av = zero;
