@@ -339,10 +339,11 @@ void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long l
                           double2* Hee, long long out_bstride, const StageField* field, int nS,
                           const double2* ptab = nullptr) {
     const int grid = std::min(nplanes, h->plane_grid);
-    plane_rhs_persist_kernel<COUL, MASK, MAXT><<<grid, h->plane_cfg.threads, h->Nk * sizeof(double2), h->stream>>>(
-        in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
-        1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0, ptab,
-        h->ntab);
+    plane_rhs_persist_kernel<COUL, MASK, MAXT>
+        <<<grid, h->plane_cfg.threads, h->Nk * sizeof(double2) + 16, h->stream>>>(
+            in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
+            1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0, ptab,
+            h->ntab, h->flag);
 }
 
 // fuse: with HSEX and a sparse model, Hee receives the whole Hamiltonian
@@ -1129,7 +1130,7 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
         h->plane_grid = 2 * std::max(nsm, 1);
     }
     {
-        const int ps = h->Nk * (int)sizeof(double2);
+        const int ps = h->Nk * (int)sizeof(double2) + 16;  // the plane and its load barrier
         if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadix89, 384>, ps))) return bail(rc);
         if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadix89, 384>, ps))) return bail(rc);
         if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadixAll, 256>, ps))) return bail(rc);

@@ -12,6 +12,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "fft_plane.cuh"
+#include "tma.cuh"
 
 namespace edus {
 
@@ -222,11 +223,20 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     const double2* __restrict__ roots, const double* __restrict__ rpos, PlanePlan pl, int nb, double inv_nk,
     double2* __restrict__ scratch, int nplanes, const int* __restrict__ hpos, const double2* __restrict__ hval,
     int nS, const int* __restrict__ opos, const double2* __restrict__ oval, int nO,
-    const double2* __restrict__ ptab = nullptr, int ntab = 0) {
+    const double2* __restrict__ ptab = nullptr, int ntab = 0, int* status = nullptr) {
     extern __shared__ double2 smem[];
     const int Nk = pl.Nk;
     const int P = nb * nb;
     double2* X = smem;
+    // the plane arrives by bulk copies (one thread issues them, one instruction
+    // per 32 KB), completion counted on the mbarrier after the plane
+    unsigned long long* lbar = (unsigned long long*)(X + Nk);
+    int nload = 0;
+    if (threadIdx.x == 0) {
+        mbar_init(lbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
     double2* slot = scratch + (long long)blockIdx.x * Nk;
     const int n1 = pl.ax[1].n, n2 = pl.ax[2].n;
     const double* rp0 = rpos + pl.ax[0].rposoff;
@@ -266,8 +276,25 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
             continue;
         }
         const double2* src = rho + (long long)b * batch_stride_in + (long long)p * Nk;
-        for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
-        __syncthreads();
+        {
+            const unsigned bytes = (unsigned)Nk * 16u;
+            if (threadIdx.x == 0) {
+                mbar_expect_tx(lbar, bytes);
+                for (unsigned off = 0; off < bytes; off += 32768u)
+                    bulk_load((unsigned char*)X + off, (const unsigned char*)src + off, min(32768u, bytes - off),
+                              lbar);
+            }
+            const bool ok = mbar_wait(lbar, (unsigned)(nload & 1), 1 << 22);
+            ++nload;
+            if (__syncthreads_or(!ok)) {
+                // give up: report, and let the copy land before the CTA ends
+                if (threadIdx.x == 0) {
+                    if (status) atomicOr(status, 1);
+                    mbar_wait(lbar, (unsigned)((nload - 1) & 1), 1 << 22);
+                }
+                return;
+            }
+        }
         plane_forward<1, MASK>(X, 0, pl, roots);
         const StageField F = field[b];
         const int n = p / nb, m = p - (p / nb) * nb;
@@ -314,7 +341,9 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
             double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
             for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = X[i];
         }
-        __syncthreads();  // X is reloaded by the next plane
+        // X is reloaded by the next plane's bulk copy: order this thread's accesses first
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
     }
 }
 

@@ -1,5 +1,5 @@
 // Tensor-memory-accelerator copies and mbarrier hand-overs used by the
-// persistent commutator (comm_ws.cuh).
+// persistent commutator (comm_ws.cuh) and the persistent plane kernel.
 //
 // A wait on an mbarrier gives up after a bounded number of polls and reports
 // false; the caller then records an error for the host (EDUS_ERR_TIMEOUT)
@@ -53,6 +53,15 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
         "[%6];\n" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(0), "r"(0), "r"(b), "r"(smem_u32(bar))
         : "memory");
+}
+
+// Untiled bulk copy global -> shared (no multicast): addresses 16-byte aligned,
+// size a multiple of 16 bytes, completion counted in bytes on `bar`.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(reinterpret_cast<unsigned long long>(src)), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 }  // namespace edus
