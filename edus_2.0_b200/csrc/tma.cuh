@@ -64,4 +64,17 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
                  : "memory");
 }
 
+// Untiled bulk copy shared -> global in the issuing thread's bulk group; the
+// thread commits the group and waits for its reads of shared memory (before
+// the buffer is reused) or for its completion (before the CTA ends).
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(
+                     reinterpret_cast<unsigned long long>(dst)),
+                 "r"(smem_u32(src)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+
 }  // namespace edus
