@@ -42,10 +42,12 @@
 // fragment-layout stores and the update warps' reads free of bank conflicts.  A product tile past the last k point (Nk = 1 mod 4) is copied
 // as zeros and its results are not written.
 //
-// Per k step and k point the products are 8 m8n8k4 (H rho - rho H from real
-// and imaginary parts).  Forming each complex product from three real ones
-// (six per k step) gained 2% of this kernel's time: the copies, not the
-// products, bound it.
+// Each complex product is formed from three real ones,
+//   Re(XY) = XrYr - XiYi,  Im(XY) = (Xr + Xi)(Yr + Yi) - XrYr - XiYi,
+// so H rho - rho H takes six m8n8k4 per k step and k point instead of eight:
+// A = Hr rr - qr hr, B = Hi ri - qi hi, D = (Hr + Hi)(rr + ri) - (qr + qi)(hr + hi)
+// accumulate, and C = (A - B, D - A - B).  The rounding differs from the
+// four-product form at the 1e-16 level of the operands' magnitudes.
 // Reference: BlockMatrix_definitions.hpp:203-226 (commutator),
 // Coulomb.cpp:151-159 (Hartree), DESolver.hpp:154-220 (stage updates).
 #pragma once
@@ -228,12 +230,12 @@ __global__ void __launch_bounds__(32 * (2 + 2 * (TILES == 3 ? 8 : 4)), 1)
             const double2* Rm = (const double2*)(ms + g.mop_bytes);
             const double2* hh = (const double2*)(ms + g.hh_off);
             const int arow = ti * 8 + ar, bcol = tj * 8 + ar;
-            // accumulators per k point: real and imaginary parts of the two C elements
-            double c0[2][2], c1[2][2];
+            // accumulators per k point: A = Re-Re, B = Im-Im, D = sum products
+            double c0[2][3], c1[2][3];
 #pragma unroll
             for (int kk = 0; kk < 2; ++kk)
 #pragma unroll
-                for (int r = 0; r < 2; ++r) c0[kk][r] = c1[kk][r] = 0.0;
+                for (int r = 0; r < 3; ++r) c0[kk][r] = c1[kk][r] = 0.0;
 #pragma unroll
             for (int ks = 0; ks < NBP / 4; ++ks) {
                 const int kc = ks * 4 + ac;
@@ -258,16 +260,12 @@ __global__ void __launch_bounds__(32 * (2 + 2 * (TILES == 3 ? 8 : 4)), 1)
 #pragma unroll
                 for (int kk = 0; kk < 2; ++kk) {
                     const double2 ha = hA[kk], qa = qA[kk], rb = rB[kk], hb = hB[kk];
-                    // H rho
                     dmma(c0[kk][0], c1[kk][0], ha.x, rb.x);
-                    dmma(c0[kk][0], c1[kk][0], -ha.y, rb.y);
-                    dmma(c0[kk][1], c1[kk][1], ha.x, rb.y);
-                    dmma(c0[kk][1], c1[kk][1], ha.y, rb.x);
-                    // - rho H
                     dmma(c0[kk][0], c1[kk][0], -qa.x, hb.x);
-                    dmma(c0[kk][0], c1[kk][0], qa.y, hb.y);
-                    dmma(c0[kk][1], c1[kk][1], -qa.x, hb.y);
-                    dmma(c0[kk][1], c1[kk][1], -qa.y, hb.x);
+                    dmma(c0[kk][1], c1[kk][1], ha.y, rb.y);
+                    dmma(c0[kk][1], c1[kk][1], -qa.y, hb.y);
+                    dmma(c0[kk][2], c1[kk][2], ha.x + ha.y, rb.x + rb.y);
+                    dmma(c0[kk][2], c1[kk][2], -(qa.x + qa.y), hb.x + hb.y);
                 }
             }
             // this tile's C slot must have been read for the previous update tile
@@ -284,7 +282,9 @@ __global__ void __launch_bounds__(32 * (2 + 2 * (TILES == 3 ? 8 : 4)), 1)
                     const double2 dh = csub(hh[row], hh[col]);
 #pragma unroll
                     for (int kk = 0; kk < 2; ++kk) {
-                        double2 c = make_double2(qq ? c1[kk][0] : c0[kk][0], qq ? c1[kk][1] : c0[kk][1]);
+                        const double xa = qq ? c1[kk][0] : c0[kk][0], xb = qq ? c1[kk][1] : c0[kk][1];
+                        const double xd = qq ? c1[kk][2] : c0[kk][2];
+                        double2 c = make_double2(xa - xb, xd - xa - xb);
                         c = cadd(c, cmul(dh, Rm[(row * W + col) * TK + kk]));
                         Cs[kk * g.CR + row * g.CW + col] = c;
                     }
