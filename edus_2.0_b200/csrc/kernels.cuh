@@ -210,9 +210,9 @@ __global__ void __launch_bounds__(MAXT) plane_rhs_kernel(
 // ---------------------------------------------------------------------------
 // Persistent single-buffer plane kernel: the same contract as plane_rhs_kernel
 // with one plane (16 Nk bytes) of shared memory, so two CTAs share an SM and
-// one CTA's transforms overlap the other's loads and stores.  The plane comes
-// in, and G and H go out, by bulk copies that one thread issues; the next copy
-// into the buffer waits for the previous store's reads of it.  CTA c works on
+// one CTA's transforms overlap the other's loads and stores.  Planes of 4096
+// points and more come in, and G and H go out, by bulk copies that one thread
+// issues; the next copy into the buffer waits for the previous store's reads.  CTA c works on
 // planes w = c, c + gridDim.x, ... of the P x B planes.  With HSEX the two
 // inverse transforms run in turn from one buffer; rho(R) survives the first
 // in the CTA's own slot of `scratch` ([gridDim.x][Nk], written and read back
@@ -234,6 +234,9 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     // per 32 KB), completion counted on the mbarrier after the plane
     unsigned long long* lbar = (unsigned long long*)(X + Nk);
     int nload = 0;
+    // small planes load and store per thread: a bulk copy's fixed latency and the
+    // barrier round trip cost more than they save there
+    const bool bulk = Nk >= 4096;
     if (threadIdx.x == 0) {
         mbar_init(lbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -278,7 +281,10 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
             continue;
         }
         const double2* src = rho + (long long)b * batch_stride_in + (long long)p * Nk;
-        {
+        if (!bulk) {
+            for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
+            __syncthreads();
+        } else {
             const unsigned bytes = (unsigned)Nk * 16u;
             if (threadIdx.x == 0) {
                 bulk_wait_read();  // the previous plane's stores have left X
@@ -316,16 +322,20 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
         __syncthreads();
         plane_inverse<1, MASK>(X, 0, pl, roots);
         double2* gdst = G_out + (long long)b * batch_stride_out + (long long)p * Nk;
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const unsigned bytes = (unsigned)Nk * 16u;
-            for (unsigned off = 0; off < bytes; off += 32768u)
-                bulk_store((unsigned char*)gdst + off, (const unsigned char*)X + off, min(32768u, bytes - off));
-            bulk_commit();
+        if (!bulk) {
+            for (int i = threadIdx.x; i < Nk; i += blockDim.x) gdst[i] = X[i];
+        } else {
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const unsigned bytes = (unsigned)Nk * 16u;
+                for (unsigned off = 0; off < bytes; off += 32768u)
+                    bulk_store((unsigned char*)gdst + off, (const unsigned char*)X + off, min(32768u, bytes - off));
+                bulk_commit();
+            }
         }
         if (COUL) {
-            if (threadIdx.x == 0) bulk_wait_read();
+            if (bulk && threadIdx.x == 0) bulk_wait_read();
             __syncthreads();  // the store above has read X before it is refilled
             if (nO > 0) {
                 // the Fock term is given (values on nO lattice vectors, zero elsewhere)
@@ -350,13 +360,18 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
             }
             plane_inverse<1, MASK>(X, 0, pl, roots);
             double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                const unsigned bytes = (unsigned)Nk * 16u;
-                for (unsigned off = 0; off < bytes; off += 32768u)
-                    bulk_store((unsigned char*)hdst + off, (const unsigned char*)X + off, min(32768u, bytes - off));
-                bulk_commit();
+            if (!bulk) {
+                for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = X[i];
+            } else {
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    const unsigned bytes = (unsigned)Nk * 16u;
+                    for (unsigned off = 0; off < bytes; off += 32768u)
+                        bulk_store((unsigned char*)hdst + off, (const unsigned char*)X + off,
+                                   min(32768u, bytes - off));
+                    bulk_commit();
+                }
             }
         }
         // X is reloaded by the next plane's bulk copy: order this thread's accesses first
