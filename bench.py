@@ -9,8 +9,10 @@ all solves and ranks (each rank runs its own independent solves: the single
 solve does not shard, so N > 1 runs replicas, weak scaling).
 
 --impl reference times the reference's CPU propagation of the same workload
-on the host cores.  The reference needs MKL/FFTW/MPI, which this image lacks,
-so that arm runs the FP64 CPU restatement in oracle/ (kind "port").
+on the host cores: the reference's own sources compiled by oracle/build_ref.py
+against the project's MPI / FFTW / MKL stand-ins (oracle/_ref/EDUS, kind
+"reference"), with the FP64 CPU restatement in oracle/ (kind "port") only when
+that binary was not built.
 """
 from __future__ import annotations
 
@@ -313,13 +315,74 @@ def run_ours(args, rank, world, local_rank):
     return result
 
 
-def cpu_baseline(inp, steps=2, threads=None):
-    """The FP64 CPU restatement (oracle/) timed on the host cores on a bounded
-    sample: `steps` RK4 steps of the same workload inside the pulse."""
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "EDUS")
+
+
+def reference_input(inp: dict, nsteps: int) -> dict:
+    """The workload as the reference's input.json: same model, grid, HSEX, RK4
+    and dt; the reference has only the sin^2 pulse, so the Gaussian pulse
+    becomes a sin^2 pulse of the same photon energy and peak field, on from
+    t = 0 (the cost of a step does not depend on the field's value).  Every
+    observable print is off after step 0 (printresolution >= steps)."""
+    L = inp["lasers"][0]
+    dt = inp["dt"]
+    return {
+        "tb_file": inp["tb_file"], "grid": inp["grid"], "filledbands": inp["filledbands"],
+        "coulomb": inp["coulomb"], "epsilon": inp["epsilon"], "r0": inp["r0"], "r0_units": inp["r0_units"],
+        "dt": dt, "dt_units": inp["dt_units"], "initialtime": 0, "initialtime_units": "femtoseconds",
+        "finaltime": dt * (nsteps - 2) + 0.5 * dt, "finaltime_units": inp["dt_units"],
+        "solver": "RK", "order": 4, "printresolution": nsteps + 10, "printresolution_pulse": nsteps + 10,
+        "lasers": [{"intensity": L["intensity"], "intensity_units": L["intensity_units"],
+                    "frequency": L["frequency"], "frequency_units": L["frequency_units"],
+                    "polarization": L["polarization"], "cycles": 10, "t0": 0.0, "t0_units": "fs"}],
+    }
+
+
+def _reference_propagate_seconds(inp: dict, nsteps: int, threads: int, workdir: str) -> float:
+    """Run oracle/_ref/EDUS for `nsteps` steps; return its own timer of
+    Simulation::Propagate (rt_graph, printed at exit) in seconds."""
+    d = os.path.join(workdir, f"steps{nsteps}")
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "input.json"), "w") as f:
+        json.dump(reference_input(inp, nsteps), f)
+    r = subprocess.run([REF_EXE, "input.json"], cwd=d, capture_output=True, text=True,
+                       env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+    if r.returncode != 0:
+        raise RuntimeError(f"reference exited with {r.returncode}: {r.stderr[-500:]}")
+    for line in r.stdout.splitlines():
+        if "Simulation::Propagate" in line:
+            parts = line.split()
+            k = parts.index("Simulation::Propagate") if "Simulation::Propagate" in parts else 1
+            val, unit = float(parts[k + 2]), parts[k + 3]
+            return val * {"s": 1.0, "ms": 1e-3, "us": 1e-6, "ns": 1e-9}[unit]
+    raise RuntimeError("reference printed no Simulation::Propagate timing")
+
+
+def reference_rate(inp: dict, steps: int, warmup: int, threads: int) -> tuple[float, float]:
+    """Steps/s of the reference build: two runs of warmup and warmup + steps
+    RK4 steps; the difference of their Propagate timers is the time of `steps`
+    steps after `warmup` (set-up, and the one observable print at step 0, cancel)."""
+    with tempfile.TemporaryDirectory() as d:
+        t_w = _reference_propagate_seconds(inp, warmup + 2, threads, d)
+        t_all = _reference_propagate_seconds(inp, warmup + 2 + steps, threads, d)
+    dt = max(t_all - t_w, 1e-9)
+    return steps / dt, dt
+
+
+def cpu_baseline(inp, steps=20, threads=None):
+    """The reference's own CPU propagation (oracle/_ref/EDUS) timed on the
+    host cores on a bounded sample of the same workload; the FP64 CPU
+    restatement (oracle/) only when that binary was not built."""
+    threads = threads or os.cpu_count()
+    if os.path.exists(REF_EXE):
+        v, dt = reference_rate(inp, steps, 1, threads)
+        return {"value": round(v, 5), "unit": "steps/s", "cores": threads, "kind": "reference",
+                "sample": f"{steps} RK4 steps of the full {WORKLOAD} workload (72x72, nb=22, HSEX) after 1 "
+                          f"warm-up step, {dt:.1f} s by the reference's Simulation::Propagate timer; reference "
+                          f"sources with the project's MPI/FFTW/MKL stand-ins, OpenMP {threads} threads"}
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
 
-    threads = threads or os.cpu_count()
     os.environ["OMP_NUM_THREADS"] = str(threads)
     cfg = pyoracle.load_input(inp)
     cfg.solver, cfg.order = 1, 4
@@ -331,38 +394,46 @@ def cpu_baseline(inp, steps=2, threads=None):
     dt = time.perf_counter() - t
     return {"value": round(steps / dt, 5), "unit": "steps/s", "cores": threads, "kind": "port",
             "sample": f"{steps} RK4 steps of the full {WORKLOAD} workload (72x72, nb=22, HSEX), "
-                      f"{dt:.1f} s, OpenMP {threads} threads"}
+                      f"{dt:.1f} s, OpenMP {threads} threads (oracle/_ref/EDUS not built)"}
 
 
 def run_reference(args):
     """--impl reference: the reference's CPU propagation on the host cores."""
     cache = os.environ.get("EDUS_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "edus_bench_tmd22"))
     inp = workload_input(cache)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle
-
     threads = os.cpu_count()
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    cfg = pyoracle.load_input(inp)
-    cfg.solver, cfg.order = 1, 4
-    o = pyoracle.Oracle(cfg)
-    o.time = cfg.lasers[0].t0 - 2.0 * cfg.lasers[0].fwhm
     K = max(1, min(args.steps, args.ref_max_steps))
-    W = min(args.warmup, 1)
-    o.step(W)
-    t = time.perf_counter()
-    o.step(K)
-    dt = time.perf_counter() - t
-    v = K / dt
+    W = args.warmup
+    if os.path.exists(REF_EXE):
+        v, dt = reference_rate(inp, K, W, threads)
+        kind = "reference"
+        sample = (f"{K} RK4 steps after {W} warm-up steps of the full workload, {dt:.1f} s by the "
+                  f"reference's own Simulation::Propagate timer (difference of a {W + 2}- and a "
+                  f"{W + 2 + K}-step run); the reference's sources built with the project's MPI (one rank), "
+                  f"FFTW and MKL stand-ins (oracle/build_ref.py), OpenMP {threads} threads")
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+        cfg = pyoracle.load_input(inp)
+        cfg.solver, cfg.order = 1, 4
+        o = pyoracle.Oracle(cfg)
+        o.time = cfg.lasers[0].t0 - 2.0 * cfg.lasers[0].fwhm
+        o.step(W)
+        t = time.perf_counter()
+        o.step(K)
+        dt = time.perf_counter() - t
+        v = K / dt
+        kind = "port"
+        sample = f"{K} RK4 steps (after {W} warm-up) of the full workload by the FP64 restatement (oracle/_ref/EDUS not built)"
     return {
         "metric": METRIC, "impl": "reference", "value": round(v, 5), "unit": "steps/s", "n_gpus": 0,
         "steps": K, "warmup": W, "ms_per_step": round(dt / K * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{WORKLOAD}: 22-orbital TMD-like, 72x72x1 k grid, HSEX, RK4 dt=0.005 fs",
                    "parallelism": "host cores"},
-        "cpu_baseline": {"value": round(v, 5), "unit": "steps/s", "cores": threads, "kind": "port",
-                         "sample": f"{K} RK4 steps (after {W} warm-up) of the full workload; the reference "
-                                   f"itself needs MKL/FFTW/MPI, absent here, so its FP64 restatement runs"},
+        "cpu_baseline": {"value": round(v, 5), "unit": "steps/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": round(v, 5), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -435,7 +506,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--ref-max-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["tmd22_rk4", "sweep"], default="tmd22_rk4")

@@ -330,7 +330,10 @@ class Model:
 
     def velocity(self):
         """Velocity operator v_d(k), [3][Nk][nb][nb] (Simulation.cpp:523-576):
-        -i [r_d(k), H0(k)], plus i R_d H0(R) added in R, over the cell area
+        -i [r_d(k), H0(k)], plus the gradient of H0 along axis d taken in the
+        space of the propagation's gradient (:554-556): i R_d H0(R) added in R
+        for gradient_space "R", the finite-difference stencil sum_b w b_d
+        H0(k + b) for "k" (kGradient_definitions.hpp:18-30); over the cell area
         (2-D) or volume (3-D); zero for 1-D grids, which the reference leaves
         unset."""
         N = self.grid
@@ -345,6 +348,20 @@ class Model:
             if N[2] > 1:
                 raise ValueError("perpendicular != 2 -> implement me!")
             det = abs(A[0, 0] * A[1, 1] - A[1, 0] * A[0, 1])
+        if self.cfg.gradient_space == "k":
+            shift, b, w = self.kgradient_stencil()
+            j = np.stack(np.meshgrid(np.arange(N[0]), np.arange(N[1]), np.arange(N[2]), indexing="ij"),
+                         -1).reshape(-1, 3)
+            for d in range(3):
+                c = -1j * (self.xik[d] @ self.H0k - self.H0k @ self.xik[d])
+                for s in range(len(w)):
+                    if w[s] * b[s, d] == 0.0:
+                        continue
+                    jn = (j + shift[s]) % np.array(N)
+                    kn = (jn[:, 0] * N[1] + jn[:, 1]) * N[2] + jn[:, 2]
+                    c = c + (w[s] * b[s, d]) * self.H0k[kn]
+                v[d] = c / det
+            return v
         H0R = fft_k_to_R(self.H0k, N)
         for d in range(3):
             c = -1j * (self.xik[d] @ self.H0k - self.H0k @ self.xik[d])

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <memory>
 #include "oracle_fft.hpp"
+#include "oracle_linalg.hpp"
 
 namespace oracle {
 
@@ -158,73 +159,6 @@ TbModel read_tb(const std::string& path) {
     }
     if (idx != m.nR) throw std::runtime_error("r block count mismatch");
     return m;
-}
-
-// ---------------------------------------------------------------------------
-// Hermitian eigensolver (stands in for LAPACKE_zheevd 'V','U',
-// src/Geometry/Matrix.cpp:10-23): cyclic complex Jacobi on the matrix built
-// from the upper triangle; eigenvalues ascending, eigenvectors in columns.
-void eigh(int n, const cd* Ain, double* w, cd* V) {
-    std::vector<cd> A((size_t)n * n);
-    for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) {
-            if (j >= i) A[i * n + j] = Ain[i * n + j];
-            else A[i * n + j] = std::conj(Ain[j * n + i]);
-        }
-    for (int i = 0; i < n; ++i) A[i * n + i] = A[i * n + i].real();
-    for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) V[i * n + j] = (i == j) ? 1.0 : 0.0;
-    for (int sweep = 0; sweep < 100; ++sweep) {
-        double off = 0, diag = 0;
-        for (int i = 0; i < n; ++i)
-            for (int j = 0; j < n; ++j) {
-                if (i != j) off += std::norm(A[i * n + j]);
-                else diag += std::norm(A[i * n + j]);
-            }
-        if (off <= 1e-32 * (diag + 1e-300) || off == 0.0) break;
-        for (int p = 0; p < n - 1; ++p)
-            for (int q = p + 1; q < n; ++q) {
-                cd g = A[p * n + q];
-                double ag = std::abs(g);
-                if (ag == 0.0) continue;
-                double app = A[p * n + p].real(), aqq = A[q * n + q].real();
-                cd ph = g / ag;  // e^{i phi}
-                double theta = (aqq - app) / (2.0 * ag);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-                double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-                // R = [[c, s e^{i phi}], [-s e^{-i phi}, c]] on (p,q); A <- R^H A R
-                for (int k = 0; k < n; ++k) {  // A R (columns)
-                    cd akp = A[k * n + p], akq = A[k * n + q];
-                    A[k * n + p] = c * akp - s * std::conj(ph) * akq;
-                    A[k * n + q] = s * ph * akp + c * akq;
-                }
-                for (int k = 0; k < n; ++k) {  // R^H A (rows)
-                    cd apk = A[p * n + k], aqk = A[q * n + k];
-                    A[p * n + k] = c * apk - s * ph * aqk;
-                    A[q * n + k] = s * std::conj(ph) * apk + c * aqk;
-                }
-                A[p * n + q] = 0.0;
-                A[q * n + p] = 0.0;
-                A[p * n + p] = app - t * ag;
-                A[q * n + q] = aqq + t * ag;
-                for (int k = 0; k < n; ++k) {
-                    cd vkp = V[k * n + p], vkq = V[k * n + q];
-                    V[k * n + p] = c * vkp - s * std::conj(ph) * vkq;
-                    V[k * n + q] = s * ph * vkp + c * vkq;
-                }
-            }
-    }
-    std::vector<int> order(n);
-    for (int i = 0; i < n; ++i) order[i] = i;
-    std::vector<double> ev(n);
-    for (int i = 0; i < n; ++i) ev[i] = A[i * n + i].real();
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ev[a] < ev[b]; });
-    std::vector<cd> Vs((size_t)n * n);
-    for (int j = 0; j < n; ++j) {
-        w[j] = ev[order[j]];
-        for (int i = 0; i < n; ++i) Vs[i * n + j] = V[i * n + order[j]];
-    }
-    std::copy(Vs.begin(), Vs.end(), V);
 }
 
 // ---------------------------------------------------------------------------
@@ -620,8 +554,11 @@ Sim* build(const oracle_cfg* cfg) {
         s.DM0R.resize(s.S());
         s.fft.run(s.rho.data(), s.DM0R.data(), -1);  // Simulation.cpp:180-181
     }
-    // velocity operator (Simulation.cpp:523-576): v = -i[r,H0]_k, then
-    // (R space) += i R_d H0(R), back to k, / |det A| (2-D) or det (3-D)
+    // velocity operator (Simulation.cpp:523-576): v = -i[r,H0]_k, then the
+    // gradient of H0 along axis d in the space of propagation of the gradient
+    // (:554-556): gradient_space "R": (R space) += i R_d H0(R) and back to k;
+    // gradient_space "k": += sum_b w_b b_d H0(k + b) (kGradient_definitions.hpp:18-30
+    // with direction e_d); then / |det A| (2-D) or det (3-D)
     if (s.dims >= 2) {
         double det;
         if (s.dims == 3) {
@@ -642,12 +579,26 @@ Sim* build(const oracle_cfg* cfg) {
                 matmul(nb, r, h, o, -im, 0.);
                 matmul(nb, h, r, o, im, 1.);
             }
-            s.fft.run(s.vel[d].data(), vR.data(), -1);
-            for (int iR = 0; iR < Nk; ++iR) {
-                double Rd = s.Rcart[3 * (size_t)iR + d];
-                for (int p = 0; p < P; ++p) vR[(size_t)iR * P + p] += 1. * im * Rd * s.H0R[(size_t)iR * P + p];
+            if (s.gw.empty()) {
+                s.fft.run(s.vel[d].data(), vR.data(), -1);
+                for (int iR = 0; iR < Nk; ++iR) {
+                    double Rd = s.Rcart[3 * (size_t)iR + d];
+                    for (int p = 0; p < P; ++p) vR[(size_t)iR * P + p] += 1. * im * Rd * s.H0R[(size_t)iR * P + p];
+                }
+                s.fft.run(vR.data(), s.vel[d].data(), +1);
+            } else {
+                for (int ik = 0; ik < Nk; ++ik) {
+                    const int j[3] = {ik / (s.N[1] * s.N[2]), (ik / s.N[2]) % s.N[1], ik % s.N[2]};
+                    for (size_t i = 0; i < s.gw.size(); ++i) {
+                        const double c = s.gw[i] * s.gvec[i][d];
+                        if (c == 0.) continue;
+                        const int jn[3] = {(j[0] + s.gshift[i][0]) % s.N[0], (j[1] + s.gshift[i][1]) % s.N[1],
+                                           (j[2] + s.gshift[i][2]) % s.N[2]};
+                        const size_t kn = ((size_t)jn[0] * s.N[1] + jn[1]) * s.N[2] + jn[2];
+                        for (int p = 0; p < P; ++p) s.vel[d][(size_t)ik * P + p] += c * s.H0k[kn * P + p];
+                    }
+                }
             }
-            s.fft.run(vR.data(), s.vel[d].data(), +1);
             for (auto& x : s.vel[d]) x /= det;
         }
     }

@@ -7,7 +7,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE = "/root/reference"
+# the reference sources, where they are mounted (no default: tests needing them skip)
+REFERENCE = os.environ.get("EDUS_REFERENCE_DIR", "")
 
 
 def pytest_configure(config):
@@ -30,7 +31,7 @@ def po():
 
 
 def reference_available() -> bool:
-    return os.path.isdir(os.path.join(REFERENCE, "src"))
+    return bool(REFERENCE) and os.path.isdir(os.path.join(REFERENCE, "src"))
 
 
 @pytest.fixture(scope="session")

@@ -1,5 +1,6 @@
 """Copy the reference's own golden vectors for the propagation path into
-tests/golden/ (run once, in a container where the reference is mounted).
+tests/golden/ (run once, where the reference is mounted; its directory is the first
+argument or EDUS_REFERENCE_DIR).
 
 Sources (gcistaro/EDUS_2.0):
   ci-test/outputs/hBN/{Population,Velocity,Laser,Time}.txt
@@ -14,7 +15,9 @@ import os
 import shutil
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("EDUS_REFERENCE_DIR", "")
+if not os.path.isdir(os.path.join(REF, "ci-test")):
+    raise SystemExit("usage: make_golden.py <reference dir> (or set EDUS_REFERENCE_DIR)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 os.makedirs(os.path.join(HERE, "hBN"), exist_ok=True)

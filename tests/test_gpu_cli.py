@@ -4,6 +4,10 @@
   writes Population.txt, Velocity.txt, Laser.txt and Time.txt that match the
   reference's outputs at ci-test/compare.py's 1e-10 (Time.txt is printed with
   6 significant digits);
+* cli.run on every case of tests/golden/ref_cases.py (HSEX, RK4 / AB4 / AB5,
+  even and odd grids, 2 to 13 bands, the k-space gradient, the Peierls gauge)
+  writes Population.txt, Population_wannier.txt and Velocity.txt that match the
+  outputs of the reference's own propagator (tests/golden/ref/) at 1e-10;
 * edus_observables equals the populations and velocity computed on the host
   from the state, the eigenvectors and the velocity operator.
 """
@@ -47,6 +51,39 @@ def test_cli_reproduces_hbn_goldens(pkg, hbn_golden_model, tmp_path):
     cum = np.concatenate([[np.zeros(3)], np.cumsum(0.5 * (Ef[1:] + Ef[:-1]) * np.diff(fine)[:, None], axis=0)])
     ref_A = -cum[::64]
     assert np.abs(A - ref_A).max() < 1e-6 * max(np.abs(ref_A).max(), 1e-30)
+
+
+def _ref_cases():
+    import sys
+
+    sys.path.insert(0, GOLDEN)
+    import ref_cases
+
+    return ref_cases
+
+
+@pytest.mark.parametrize("name", sorted(_ref_cases().CASES))
+def test_cli_reproduces_reference_outputs(pkg, tmp_path, name):
+    """The GPU product against the reference's own propagator on the same input."""
+    rc = _ref_cases()
+    case = rc.CASES[name]
+    seed = rc.write_model(pkg.workloads, case, str(tmp_path))
+    meta = json.load(open(os.path.join(GOLDEN, "ref", name, "meta.json")))
+    assert rc.sha256(seed + "_tb.dat") == meta["model_sha256"]
+    path = os.path.join(str(tmp_path), "input.json")
+    with open(path, "w") as f:
+        json.dump(rc.make_input(case, seed), f)
+    out = os.path.join(str(tmp_path), "Output")
+    from edus_b200 import cli
+
+    n = cli.run(path, out)
+    assert n == case["nsteps"]
+    for fn in ("Population.txt", "Population_wannier.txt", "Velocity.txt"):
+        got = np.loadtxt(os.path.join(out, fn))
+        ref = np.loadtxt(os.path.join(GOLDEN, "ref", name, fn))
+        assert got.shape == ref.shape, fn
+        err = np.abs(got - ref).max()
+        assert err < 1e-10, f"{name} {fn}: max |GPU - reference| = {err:.3e}"
 
 
 def test_observables_match_host(pkg, tmp_path):
