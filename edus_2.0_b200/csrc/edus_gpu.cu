@@ -939,12 +939,20 @@ __global__ void gather_R_kernel(const double2* __restrict__ planes, const int* _
     }
 }
 
-// Device status word: a bounded wait that ran out inside a kernel sets it.
+// Device status word: a bounded wait that ran out inside a kernel sets it
+// (the TMA commutator's operand hand-over, the plane kernel's bulk load).  It
+// is cleared once reported, so the handle stays usable: the results of the
+// calls since the last check are not to be trusted, later calls are.
 int check_status(edus_handle* h) {
     int v = 0;
     CU(h, cudaMemcpyAsync(&v, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CU(h, cudaStreamSynchronize(h->stream));
-    if (v) return fail(h, EDUS_ERR_TIMEOUT, "a bounded wait for tensor copies in the commutator ran out");
+    if (v) {
+        CU(h, cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+        return fail(h, EDUS_ERR_TIMEOUT,
+                    "a bounded wait in a kernel ran out (commutator_ws_kernel operand hand-over or "
+                    "plane_rhs_persist_kernel bulk load): the results since the last synchronising call are invalid");
+    }
     return EDUS_OK;
 }
 

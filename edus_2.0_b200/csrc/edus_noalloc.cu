@@ -15,12 +15,21 @@
 //
 // Rules for users:
 //  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress) and sets the kernels' shared-memory limits; make
-//    that first call before any stream capture on that device;
+//    (cudaGetSymbolAddress), sets the kernels' shared-memory limits and copies
+//    the k grid's FFT tables from host memory into the array (then waits for
+//    that copy); make that first call before any stream capture on that
+//    device.  A call whose k grid differs from the previous call's on that
+//    device copies the new grid's tables the same way; every other call only
+//    queues kernels (the field of the evaluation travels as a kernel
+//    argument);
 //  * all calls share the one array: calls that overlap on the GPU (different
 //    streams, or several host threads) race on it -- serialise them;
 //  * problems whose intermediates exceed the array are rejected with
-//    EDUS_ERR_UNSUPPORTED; nothing here calls cudaMalloc or cudaFree.
+//    EDUS_ERR_UNSUPPORTED; nothing here calls cudaMalloc or cudaFree;
+//  * W must be real (the screened potential has no imaginary part): a W_R
+//    whose imaginary part is not zero is refused on the device, where the
+//    check runs, by an output of NaN (an error code would need a
+//    synchronisation).
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -48,6 +57,7 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 void* g_scratch_addr[kMaxDevices] = {nullptr};
 int g_smem_set[kMaxDevices] = {0};  // plane-kernel dynamic smem limit already raised to this many bytes
+int g_tab_grid[kMaxDevices][3] = {};  // k grid whose FFT tables sit at the front of the array (0: none)
 thread_local char* g_errbuf = nullptr;
 thread_local int g_errlen = 0;
 
@@ -77,18 +87,51 @@ __global__ void prep_hamiltonian(const double2* __restrict__ H0, const double2* 
 // digit-reversed positions of the plane FFT; rho0_nn(R=0) into r0diag.
 __global__ void prep_hsex(const double2* __restrict__ W, const double2* __restrict__ rho0, double* __restrict__ Wp,
                           double2* __restrict__ r0p, double2* __restrict__ r0diag, const int* __restrict__ fq0,
-                          const int* __restrict__ fq1, const int* __restrict__ fq2, int N1, int N2, int Nk, int nb) {
+                          const int* __restrict__ fq1, const int* __restrict__ fq2, int N1, int N2, int Nk, int nb,
+                          int* __restrict__ status) {
     const int P = nb * nb;
     const long long S = (long long)Nk * P;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < S; i += (long long)gridDim.x * blockDim.x) {
         const int p = (int)(i / Nk), pos = (int)(i - (long long)p * Nk);
         const int q2 = pos % N2, t = pos / N2, q1 = t % N1, q0 = t / N1;
         const long long iR = ((long long)fq0[q0] * N1 + fq1[q1]) * N2 + fq2[q2];
-        Wp[i] = W[iR * P + p].x;
+        const double2 w = W[iR * P + p];
+        Wp[i] = w.x;
+        if (w.y != 0.0) *status = 1;  // refused: the output becomes NaN
         r0p[i] = rho0[iR * P + p];
     }
     if (blockIdx.x == 0)
         for (int n = threadIdx.x; n < nb; n += blockDim.x) r0diag[n] = rho0[n * nb + n];
+}
+
+// The evaluation's two stage fields (by value: no host copy), a cleared
+// Hartree accumulator and a cleared status word.
+__global__ void set_call_state(StageField* __restrict__ field, StageField f0, StageField f1,
+                               double2* __restrict__ diag0, int nb, int* __restrict__ status) {
+    if (threadIdx.x == 0) {
+        field[0] = f0;
+        field[1] = f1;
+        *status = 0;
+    }
+    for (int n = threadIdx.x; n < nb; n += blockDim.x) diag0[n] = make_double2(0.0, 0.0);
+}
+
+// out[k][p] = src[p][k], or NaN everywhere when the status word is set.
+__global__ void transpose_out(const double2* __restrict__ src, double2* __restrict__ dst, int Nk, int P,
+                              const int* __restrict__ status) {
+    __shared__ double2 tile[32][33];
+    const bool refused = *status != 0;
+    const int p0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int p = p0 + r, k = k0 + threadIdx.x;
+        if (k < Nk && p < P) tile[r][threadIdx.x] = src[(long long)p * Nk + k];
+    }
+    __syncthreads();
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int k = k0 + r, p = p0 + threadIdx.x;
+        if (k < Nk && p < P) dst[(long long)k * P + p] = refused ? make_double2(nan, nan) : tile[threadIdx.x][r];
+    }
 }
 
 }  // namespace
@@ -134,6 +177,10 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
         off = align256(off + bytes);
         return o;
     };
+    // the grid's tables first: they stay in place while the grid does not change
+    const size_t o_roots = take(roots.size() * sizeof(double2));
+    const size_t o_rpos = take(rpos.size() * sizeof(double));
+    const size_t o_fq = take(fqall.size() * sizeof(int));
     const size_t o_rho = take(S * sizeof(double2));
     const size_t o_G = take(S * sizeof(double2));
     const size_t o_out = take(S * sizeof(double2));
@@ -141,12 +188,10 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
     const size_t o_Hee = coulomb ? take(S * sizeof(double2)) : 0;
     const size_t o_r0p = coulomb ? take(S * sizeof(double2)) : 0;
     const size_t o_Wp = coulomb ? take(S * sizeof(double)) : 0;
-    const size_t o_roots = take(roots.size() * sizeof(double2));
-    const size_t o_rpos = take(rpos.size() * sizeof(double));
-    const size_t o_fq = take(fqall.size() * sizeof(int));
     const size_t o_field = take(2 * sizeof(StageField));
     const size_t o_diag0 = take(nb * sizeof(double2));
     const size_t o_r0diag = take(nb * sizeof(double2));
+    const size_t o_status = take(sizeof(int));
     if (off > (size_t)EDUS_NOALLOC_SCRATCH_BYTES)
         return nfail(EDUS_ERR_UNSUPPORTED, "edus_rhs_noalloc: this grid and band count need " + std::to_string(off) +
                                                " bytes of scratch; the built-in array holds " +
@@ -202,6 +247,7 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
     StageField* d_field = (StageField*)(base + o_field);
     double2* diag0 = (double2*)(base + o_diag0);
     double2* r0diag = (double2*)(base + o_r0diag);
+    int* d_status = (int*)(base + o_status);
 
     // field: the plane kernel needs g = A^T E for R.E; the Hamiltonian's E.xi
     // is folded into H1 here, so the commutator sees E = 0
@@ -216,14 +262,25 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
         cudaError_t e_ = (expr);                                                           \
         if (e_ != cudaSuccess) return nfail(EDUS_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
     } while (0)
-    // tables (pageable sources: each copy has left the host buffer on return)
-    NA_CU(cudaMemcpyAsync(d_roots, roots.data(), roots.size() * sizeof(double2), cudaMemcpyHostToDevice, stream));
-    NA_CU(cudaMemcpyAsync(d_rpos, rpos.data(), rpos.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-    NA_CU(cudaMemcpyAsync(d_fq, fqall.data(), fqall.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
-    NA_CU(cudaMemcpyAsync(d_field, hf, sizeof(hf), cudaMemcpyHostToDevice, stream));
-    // diag0 is read only after the plane kernel writes it; cleared so that a
-    // stale value from an earlier call can never leak into this one
-    NA_CU(cudaMemsetAsync(diag0, 0, nb * sizeof(double2), stream));
+    // the grid's FFT tables: copied only when the device's resident tables are
+    // for another grid (first call, or a new grid), and waited for, so that no
+    // later call depends on a copy in flight
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        if (g_tab_grid[dev][0] != N[0] || g_tab_grid[dev][1] != N[1] || g_tab_grid[dev][2] != N[2]) {
+            g_tab_grid[dev][0] = 0;
+            NA_CU(cudaMemcpyAsync(d_roots, roots.data(), roots.size() * sizeof(double2), cudaMemcpyHostToDevice, stream));
+            NA_CU(cudaMemcpyAsync(d_rpos, rpos.data(), rpos.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+            NA_CU(cudaMemcpyAsync(d_fq, fqall.data(), fqall.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+            NA_CU(cudaStreamSynchronize(stream));
+            for (int d = 0; d < 3; ++d) g_tab_grid[dev][d] = N[d];
+        }
+    }
+    // the field by value; diag0 is read only after the plane kernel writes it,
+    // and is cleared so that a stale value from an earlier call can never leak
+    // into this one; the status word starts at zero
+    set_call_state<<<1, 64, 0, stream>>>(d_field, hf[0], hf[1], diag0, nb, d_status);
+    NA_CU(cudaGetLastError());
 
     const int nthr = 256;
     const int nblk = (int)std::min<size_t>((S + nthr - 1) / nthr, 148 * 16);
@@ -233,7 +290,8 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
                                                  efield[1], efield[2]);
     if (coulomb)
         prep_hsex<<<nblk, nthr, 0, stream>>>((const double2*)W_R, (const double2*)rho0_R, Wp, r0p, r0diag,
-                                             d_fq + fqoff[0], d_fq + fqoff[1], d_fq + fqoff[2], N[1], N[2], Nk, nb);
+                                             d_fq + fqoff[0], d_fq + fqoff[1], d_fq + fqoff[2], N[1], N[2], Nk, nb,
+                                             d_status);
     NA_CU(cudaGetLastError());
     dim3 pg(P, 1);
     if (coulomb)
@@ -274,7 +332,7 @@ extern "C" int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, cons
     }
     NA_CU(cudaGetLastError());
     dim3 tg2((P + 31) / 32, (Nk + 31) / 32);
-    transpose_pk_to_kp<<<tg2, tb, 0, stream>>>(out_pk, (double2*)out_k, Nk, P);
+    transpose_out<<<tg2, tb, 0, stream>>>(out_pk, (double2*)out_k, Nk, P, d_status);
     NA_CU(cudaGetLastError());
 #undef NA_CU
     return EDUS_OK;

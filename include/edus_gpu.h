@@ -309,11 +309,17 @@ int edus_get_profile(edus_handle* h, int kind, double* total_ms, unsigned long l
  * Returns once the work is queued.  The intermediates must fit the array
  * (about 6.5 * Nk * nb^2 * 16 bytes with coulomb, 4 * ... without); larger
  * problems get EDUS_ERR_UNSUPPORTED.  The first call on a device looks up the
- * array's address and raises the kernels' shared-memory limit: make it before
- * any stream capture on that device.  All calls share the array, and each
- * call overwrites what the last one left there: calls that overlap on the
- * GPU (several streams or host threads at once) race and must be serialised
- * by the caller. */
+ * array's address, raises the kernels' shared-memory limit and copies the k
+ * grid's FFT tables from host memory into the array, waiting for that copy:
+ * make it before any stream capture on that device.  A call whose grid
+ * differs from the previous call's on the device copies its tables the same
+ * way; other calls only queue kernels (the field goes as a kernel argument).
+ * W_R must be real, as edus_upload_model requires: the check runs on the
+ * device, so a W_R with a non-zero imaginary part is refused by an out_k
+ * filled with NaN rather than by a return code.  All calls share the array,
+ * and each call overwrites what the last one left there: calls that overlap
+ * on the GPU (several streams or host threads at once) race and must be
+ * serialised by the caller. */
 #define EDUS_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
 int edus_rhs_noalloc(const int grid[3], int nbands, int coulomb, const double lattice[9],
                      const double efield[3], const double* H0_k, const double* xi_k,

@@ -78,6 +78,11 @@ CASES = [
     ("mma14", (10, 6, 1), 14, 2, False),
     ("mma17", (8, 6, 1), 17, 2, True),
     ("mma33", (6, 4, 1), 33, 2, True),
+    # planes of 4096 points and more arrive by bulk copies; without HSEX, G
+    # leaves by a bulk store and the next plane's bulk load into the same
+    # buffer must wait for that store's reads
+    ("bulk_ipa", (72, 64, 1), 3, 2, False),
+    ("bulk_ipa_70x60", (70, 60, 1), 2, 2, False),
 ]
 
 
