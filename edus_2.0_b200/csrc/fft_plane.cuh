@@ -184,7 +184,7 @@ struct Dft<8, S, C> {
     }
 };
 
-// Generic odd radix (7) through the axis root table:
+// Generic odd radix (7, 11, 13) through the axis root table:
 // W_R^{m} = root[m * (n / R)] (conjugated for S = +1).
 template <int R, int S, typename C>
 struct DftGeneric {
@@ -208,6 +208,10 @@ struct DftGeneric {
 };
 template <int S, typename C>
 struct Dft<7, S, C> : DftGeneric<7, S, C> {};
+template <int S, typename C>
+struct Dft<11, S, C> : DftGeneric<11, S, C> {};
+template <int S, typename C>
+struct Dft<13, S, C> : DftGeneric<13, S, C> {};
 
 // Composite radix R = R1*R2 entirely in registers (four-step):
 //   y[k1 + R1 k2] = sum_n2 W_R2^{n2 k2} W_R^{n2 k1} sum_n1 x[R2 n1 + n2] W_R1^{n1 k1}
@@ -325,7 +329,7 @@ __device__ __forceinline__ void stage_R(C* buf, int bufstride, int Nk, const Axi
 
 // Radix sets a plane kernel may be specialised for (bit r set = radix r).
 constexpr int kRadixAll = (1 << 2) | (1 << 3) | (1 << 4) | (1 << 5) | (1 << 6) | (1 << 7) | (1 << 8) | (1 << 9) |
-                          (1 << 10) | (1 << 12);
+                          (1 << 10) | (1 << 11) | (1 << 12) | (1 << 13);
 constexpr int kRadix89 = (1 << 8) | (1 << 9);
 
 template <bool FWD, int NBUF, int MASK, typename C>
@@ -346,7 +350,9 @@ __device__ __forceinline__ void run_stage(C* buf, int bufstride, int Nk, const A
         EDUS_STAGE_CASE(8)
         EDUS_STAGE_CASE(9)
         EDUS_STAGE_CASE(10)
+        EDUS_STAGE_CASE(11)
         EDUS_STAGE_CASE(12)
+        EDUS_STAGE_CASE(13)
 #undef EDUS_STAGE_CASE
         default: break;  // the host never selects a kernel lacking a radix of its plan
     }

@@ -7,7 +7,7 @@ namespace edus {
 
 // Radices with an in-register DFT in fft_plane.cuh.
 inline const std::vector<int>& supported_radices() {
-    static const std::vector<int> r = {12, 10, 9, 8, 7, 6, 5, 4, 3, 2};
+    static const std::vector<int> r = {13, 12, 11, 10, 9, 8, 7, 6, 5, 4, 3, 2};
     return r;
 }
 
@@ -105,7 +105,7 @@ inline bool build_plane_plan(const int N[3], PlanePlan& plan, PlaneTables& tab, 
         stride *= A.n;
         std::vector<int> r;
         if (!choose_radices(A.n, r)) {
-            err = "grid size " + std::to_string(A.n) + " has a prime factor other than 2, 3, 5, 7";
+            err = "grid size " + std::to_string(A.n) + " has a prime factor other than 2, 3, 5, 7, 11, 13";
             return false;
         }
         A.nst = (int)r.size();
