@@ -334,12 +334,12 @@ void launch_plane_variant(edus_handle* h, dim3 grid, const double2* in, long lon
         1.0 / h->Nk, h->hpos, h->hval, nS, ptab, h->ntab);
 }
 
-template <bool COUL, int MASK, int MAXT>
+template <bool COUL, int MASK, int MAXT, int BT = 1>
 void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long long in_bstride, double2* G,
                           double2* Hee, long long out_bstride, const StageField* field, int nS,
                           const double2* ptab = nullptr) {
     const int grid = std::min(nplanes, h->plane_grid);
-    plane_rhs_persist_kernel<COUL, MASK, MAXT>
+    plane_rhs_persist_kernel<COUL, MASK, MAXT, BT>
         <<<grid, h->plane_cfg.threads, h->Nk * sizeof(double2) + 16, h->stream>>>(
             in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
             1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0, ptab,
@@ -407,18 +407,28 @@ int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double
         const int np = h->P * nbatch;
         if (h->plane_cfg.persist) {
             if (h->plane_cfg.variant == 1) {
-                if (c) launch_plane_persist<true, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
-                else launch_plane_persist<false, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+                if (c) launch_plane_persist<true, kRadix89, kPersist89Threads, kPersist89Batch>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+                else launch_plane_persist<false, kRadix89, kPersist89Threads, kPersist89Batch>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
             } else {
-                if (c) launch_plane_persist<true, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
-                else launch_plane_persist<false, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+                if (h->plane_cfg.variant == 2) {
+                    if (c) launch_plane_persist<true, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+                    else launch_plane_persist<false, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+                } else {
+                    if (c) launch_plane_persist<true, kRadixCommon, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+                    else launch_plane_persist<false, kRadixCommon, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+                }
             }
         } else if (h->plane_cfg.variant == 1) {
             if (c) launch_plane_variant<true, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
             else launch_plane_variant<false, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
         } else {
-            if (c) launch_plane_variant<true, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
-            else launch_plane_variant<false, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+            if (h->plane_cfg.variant == 2) {
+                if (c) launch_plane_variant<true, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+                else launch_plane_variant<false, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+            } else {
+                if (c) launch_plane_variant<true, kRadixCommon, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+                else launch_plane_variant<false, kRadixCommon, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, h->nS, h->ptab);
+            }
         }
         h->launches++;
         CU(h, cudaGetLastError());
@@ -467,18 +477,24 @@ int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double
     if (h->plane_cfg.persist) {
         const int np = h->P * nbatch;
         if (h->plane_cfg.variant == 1) {
-            if (c) launch_plane_persist<true, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
-            else launch_plane_persist<false, kRadix89, 384>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
-        } else {
+            if (c) launch_plane_persist<true, kRadix89, kPersist89Threads, kPersist89Batch>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
+            else launch_plane_persist<false, kRadix89, kPersist89Threads, kPersist89Batch>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
+        } else if (h->plane_cfg.variant == 2) {
             if (c) launch_plane_persist<true, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
             else launch_plane_persist<false, kRadixAll, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
+        } else {
+            if (c) launch_plane_persist<true, kRadixCommon, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
+            else launch_plane_persist<false, kRadixCommon, 256>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
         }
     } else if (h->plane_cfg.variant == 1) {
         if (c) launch_plane_variant<true, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field, nS);
         else launch_plane_variant<false, kRadix89, 768>(h, grid, in, in_bstride, G, Hee, out_bstride, field, nS);
-    } else {
+    } else if (h->plane_cfg.variant == 2) {
         if (c) launch_plane_variant<true, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, nS);
         else launch_plane_variant<false, kRadixAll, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, nS);
+    } else {
+        if (c) launch_plane_variant<true, kRadixCommon, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, nS);
+        else launch_plane_variant<false, kRadixCommon, 512>(h, grid, in, in_bstride, G, Hee, out_bstride, field, nS);
     }
     h->launches++;
     if (kmode) launch_kgrad();
@@ -1139,13 +1155,17 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     }
     {
         const int ps = h->Nk * (int)sizeof(double2) + 16;  // the plane and its load barrier
-        if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadix89, 384>, ps))) return bail(rc);
-        if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadix89, 384>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadix89, kPersist89Threads, kPersist89Batch>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadix89, kPersist89Threads, kPersist89Batch>, ps))) return bail(rc);
         if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadixAll, 256>, ps))) return bail(rc);
         if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadixAll, 256>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadixCommon, 256>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadixCommon, 256>, ps))) return bail(rc);
     }
     if ((rc = set_smem(h, plane_rhs_kernel<true, kRadixAll, 512>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_rhs_kernel<false, kRadixAll, 512>, h->smem_plane))) return bail(rc);
+    if ((rc = set_smem(h, plane_rhs_kernel<true, kRadixCommon, 512>, h->smem_plane))) return bail(rc);
+    if ((rc = set_smem(h, plane_rhs_kernel<false, kRadixCommon, 512>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_rhs_kernel<true, kRadix89, 768>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_rhs_kernel<false, kRadix89, 768>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_to_R_kernel<kRadixAll, 256>, h->Nk * (int)sizeof(double2)))) return bail(rc);
@@ -2141,7 +2161,7 @@ int edus_autotune(edus_handle* h, int* plane_threads, int* comm_tensor) {
     cudaMemcpy(df, f.data(), f.size() * sizeof(StageField), cudaMemcpyHostToDevice);
     // plane kernel: thread counts, multiples of 32 up to the variant's maximum
     {
-        const int tmax = h->plane_cfg.persist ? (h->plane_cfg.variant == 1 ? 384 : 256)
+        const int tmax = h->plane_cfg.persist ? (h->plane_cfg.variant == 1 ? kPersist89Threads : 256)
                                               : (h->plane_cfg.variant == 1 ? 768 : 512);
         const int keep = h->plane_cfg.threads;
         int best_t = keep;

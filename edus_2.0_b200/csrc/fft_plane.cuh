@@ -184,26 +184,43 @@ struct Dft<8, S, C> {
     }
 };
 
-// Generic odd radix (7, 11, 13) through the axis root table:
-// W_R^{m} = root[m * (n / R)] (conjugated for S = +1).
+// Generic odd radix (7, 11, 13) through the axis root table,
+// W_R^{m} = root[m * (n / R)] = cos(2 pi m / R) - i sin(2 pi m / R).  Inputs
+// j and R - j are paired (a_j = x_j + x_{R-j}, b_j = x_j - x_{R-j}), so that
+// with theta = 2 pi j d / R
+//   y_d     = x_0 + sum_j a_j cos(theta) + S i sum_j b_j sin(theta)
+//   y_{R-d} = x_0 + sum_j a_j cos(theta) - S i sum_j b_j sin(theta)
+// (half the products of the plain sum, and R + 3 complex registers).
 template <int R, int S, typename C>
 struct DftGeneric {
     __device__ __forceinline__ static void run(C* v, const double2* root, int n) {
-        C y[R];
+        using T = typename CplxT<C>::T;
+        constexpr int H = (R - 1) / 2;
         const int step = n / R;
+        C a[H], b[H];
+        const C x0 = v[0];
+        C y0 = x0;
 #pragma unroll
-        for (int d = 0; d < R; ++d) {
-            C s = v[0];
-#pragma unroll
-            for (int b = 1; b < R; ++b) {
-                C w = ldroot<C>(&root[((b * d) % R) * step]);
-                if (S > 0) w.y = -w.y;
-                s = cadd(s, cmul(v[b], w));
-            }
-            y[d] = s;
+        for (int j = 1; j <= H; ++j) {
+            a[j - 1] = cadd(v[j], v[R - j]);
+            b[j - 1] = csub(v[j], v[R - j]);
+            y0 = cadd(y0, a[j - 1]);
         }
+        v[0] = y0;
 #pragma unroll
-        for (int d = 0; d < R; ++d) v[d] = y[d];
+        for (int d = 1; d <= H; ++d) {
+            C A = x0, B = cmake<C>((T)0, (T)0);
+#pragma unroll
+            for (int j = 1; j <= H; ++j) {
+                const C w = ldroot<C>(&root[((j * d) % R) * step]);
+                const T c = w.x, sn = -w.y;
+                A = cmake<C>(fma(a[j - 1].x, c, A.x), fma(a[j - 1].y, c, A.y));
+                B = cmake<C>(fma(b[j - 1].x, sn, B.x), fma(b[j - 1].y, sn, B.y));
+            }
+            const C iB = cmul_si<S>(B);  // S i B
+            v[d] = cadd(A, iB);
+            v[R - d] = csub(A, iB);
+        }
     }
 };
 template <int S, typename C>
@@ -275,12 +292,39 @@ __device__ __forceinline__ void twiddle_powers(C* w, C w1) {
     }
 }
 
+// One radix-R butterfly in registers: DIF (FWD) or DIT, with the stage
+// twiddles of butterfly position a (a = 0: none).
+template <int R, bool FWD, typename C>
+__device__ __forceinline__ void butterfly_R(C* v, int a, int tw_step, int n, const double2* __restrict__ root) {
+    constexpr int S = FWD ? -1 : +1;
+    if (FWD) {
+        Dft<R, S, C>::run(v, root, n);
+        if (a != 0) {
+            C w[R];
+            twiddle_powers<R, false>(w, ldroot<C>(&root[a * tw_step]));
+#pragma unroll
+            for (int d = 1; d < R; ++d) v[d] = cmul(v[d], w[d]);
+        }
+    } else {
+        if (a != 0) {
+            C w[R];
+            twiddle_powers<R, true>(w, ldroot<C>(&root[a * tw_step]));
+#pragma unroll
+            for (int d = 1; d < R; ++d) v[d] = cmul(v[d], w[d]);
+        }
+        Dft<R, S, C>::run(v, root, n);
+    }
+}
+
 // One radix-R stage over every line of axis `ax` of the NBUF planes that
 // start at `buf[0]`, `buf[0] + bufstride`, ...  DIF when FWD, DIT otherwise.
-template <int R, bool FWD, int NBUF, typename C>
+// BT > 1: a thread takes BT butterflies at once (tasks t, t + T, ...), loads
+// all of them before the first DFT and stores after the last, so their
+// shared-memory latencies overlap (butterflies of one stage touch disjoint
+// elements, so the reordering is safe).
+template <int R, bool FWD, int NBUF, typename C, int BT = 1>
 __device__ __forceinline__ void stage_R(C* buf, int bufstride, int Nk, const AxisPlan& ax, int s,
                                         const double2* __restrict__ root) {
-    constexpr int S = FWD ? -1 : +1;
     const int n = ax.n;
     const int inner = ax.inner;
     const int L = ax.L[s];
@@ -289,98 +333,128 @@ __device__ __forceinline__ void stage_R(C* buf, int bufstride, int Nk, const Axi
     const int tw_step = n / M;
     const int ntask = Nk / R;
     const FastDiv fdi = ax.fd_inner, fdb = ax.fd_nbfly[s], fdl = ax.fd_L[s];
-    for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
-        const int tmp = fdiv(t, fdi);
-        const int in = t - tmp * inner;
-        const int o = fdiv(tmp, fdb);
-        const int bfly = tmp - o * nbfly;
-        const int blk = fdiv(bfly, fdl);
-        const int a = bfly - blk * L;
-        const int base = o * (n * inner) + in + (blk * M + a) * inner;
-        const int step = L * inner;
+    const int step = L * inner;
+    if constexpr (BT == 1) {
+        for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
+            const int tmp = fdiv(t, fdi);
+            const int in = t - tmp * inner;
+            const int o = fdiv(tmp, fdb);
+            const int bfly = tmp - o * nbfly;
+            const int blk = fdiv(bfly, fdl);
+            const int a = bfly - blk * L;
+            const int base = o * (n * inner) + in + (blk * M + a) * inner;
 #pragma unroll
-        for (int q = 0; q < NBUF; ++q) {
-            C* X = buf + q * bufstride;
-            C v[R];
+            for (int q = 0; q < NBUF; ++q) {
+                C* X = buf + q * bufstride;
+                C v[R];
 #pragma unroll
-            for (int b = 0; b < R; ++b) v[b] = X[base + b * step];
-            if (FWD) {
-                Dft<R, S, C>::run(v, root, n);
-                if (a != 0) {
-                    C w[R];
-                    twiddle_powers<R, false>(w, ldroot<C>(&root[a * tw_step]));
+                for (int b = 0; b < R; ++b) v[b] = X[base + b * step];
+                butterfly_R<R, FWD, C>(v, a, tw_step, n, root);
 #pragma unroll
-                    for (int d = 1; d < R; ++d) v[d] = cmul(v[d], w[d]);
-                }
-            } else {
-                if (a != 0) {
-                    C w[R];
-                    twiddle_powers<R, true>(w, ldroot<C>(&root[a * tw_step]));
+                for (int b = 0; b < R; ++b) X[base + b * step] = v[b];
+            }
+        }
+    } else {
+        for (int t0 = threadIdx.x; t0 < ntask; t0 += BT * blockDim.x) {
+            int base[BT], av[BT];
+            bool on[BT];
 #pragma unroll
-                    for (int d = 1; d < R; ++d) v[d] = cmul(v[d], w[d]);
-                }
-                Dft<R, S, C>::run(v, root, n);
+            for (int j = 0; j < BT; ++j) {
+                const int t = t0 + j * (int)blockDim.x;
+                on[j] = t < ntask;
+                const int tt = on[j] ? t : t0;
+                const int tmp = fdiv(tt, fdi);
+                const int in = tt - tmp * inner;
+                const int o = fdiv(tmp, fdb);
+                const int bfly = tmp - o * nbfly;
+                const int blk = fdiv(bfly, fdl);
+                av[j] = bfly - blk * L;
+                base[j] = o * (n * inner) + in + (blk * M + av[j]) * inner;
             }
 #pragma unroll
-            for (int b = 0; b < R; ++b) X[base + b * step] = v[b];
+            // a task past the end repeats task t0's loads and arithmetic and
+            // stores nothing: no branch inside the batch
+            for (int q = 0; q < NBUF; ++q) {
+                C* X = buf + q * bufstride;
+                C v[BT][R];
+#pragma unroll
+                for (int j = 0; j < BT; ++j)
+#pragma unroll
+                    for (int b = 0; b < R; ++b) v[j][b] = X[base[j] + b * step];
+#pragma unroll
+                for (int j = 0; j < BT; ++j) butterfly_R<R, FWD, C>(v[j], av[j], tw_step, n, root);
+#pragma unroll
+                for (int j = 0; j < BT; ++j)
+                    if (on[j]) {
+#pragma unroll
+                        for (int b = 0; b < R; ++b) X[base[j] + b * step] = v[j][b];
+                    }
+            }
         }
     }
 }
 
-// Radix sets a plane kernel may be specialised for (bit r set = radix r).
-constexpr int kRadixAll = (1 << 2) | (1 << 3) | (1 << 4) | (1 << 5) | (1 << 6) | (1 << 7) | (1 << 8) | (1 << 9) |
-                          (1 << 10) | (1 << 11) | (1 << 12) | (1 << 13);
+// Radix sets a plane kernel may be specialised for (bit r set = radix r):
+// every radix; the common ones (the generic odd radices 11 and 13 need many
+// registers, and plans without them run kernels compiled without them); the
+// 72-point axes.
+constexpr int kRadixCommon = (1 << 2) | (1 << 3) | (1 << 4) | (1 << 5) | (1 << 6) | (1 << 7) | (1 << 8) |
+                             (1 << 9) | (1 << 10) | (1 << 12);
+constexpr int kRadixAll = kRadixCommon | (1 << 11) | (1 << 13);
 constexpr int kRadix89 = (1 << 8) | (1 << 9);
 
-template <bool FWD, int NBUF, int MASK, typename C>
+template <bool FWD, int NBUF, int MASK, typename C, int BT = 1>
 __device__ __forceinline__ void run_stage(C* buf, int bufstride, int Nk, const AxisPlan& ax, int s,
                                           const double2* __restrict__ roots) {
     const double2* root = roots + ax.rootoff;
-    switch (ax.r[s]) {
-#define EDUS_STAGE_CASE(R)                                                                             \
-    case R:                                                                                            \
-        if constexpr ((MASK >> R) & 1) stage_R<R, FWD, NBUF, C>(buf, bufstride, Nk, ax, s, root);   \
-        break;
-        EDUS_STAGE_CASE(2)
-        EDUS_STAGE_CASE(3)
-        EDUS_STAGE_CASE(4)
-        EDUS_STAGE_CASE(5)
-        EDUS_STAGE_CASE(6)
-        EDUS_STAGE_CASE(7)
-        EDUS_STAGE_CASE(8)
-        EDUS_STAGE_CASE(9)
-        EDUS_STAGE_CASE(10)
-        EDUS_STAGE_CASE(11)
-        EDUS_STAGE_CASE(12)
-        EDUS_STAGE_CASE(13)
-#undef EDUS_STAGE_CASE
-        default: break;  // the host never selects a kernel lacking a radix of its plan
+    const int r = ax.r[s];
+    // only the radices of MASK are compiled in (the host never selects a
+    // kernel lacking a radix of its plan)
+#define EDUS_STAGE_CASE(R)                                                               \
+    if constexpr ((MASK >> R) & 1) {                                                     \
+        if (r == R) {                                                                    \
+            stage_R<R, FWD, NBUF, C, BT>(buf, bufstride, Nk, ax, s, root);               \
+            return;                                                                      \
+        }                                                                                \
     }
+    EDUS_STAGE_CASE(2)
+    EDUS_STAGE_CASE(3)
+    EDUS_STAGE_CASE(4)
+    EDUS_STAGE_CASE(5)
+    EDUS_STAGE_CASE(6)
+    EDUS_STAGE_CASE(7)
+    EDUS_STAGE_CASE(8)
+    EDUS_STAGE_CASE(9)
+    EDUS_STAGE_CASE(10)
+    EDUS_STAGE_CASE(11)
+    EDUS_STAGE_CASE(12)
+    EDUS_STAGE_CASE(13)
+#undef EDUS_STAGE_CASE
 }
 
 // Forward (k -> R, unnormalised sign -1) transform of the plane(s) in place.
-template <int NBUF, int MASK, typename C>
-__device__ void plane_forward(C* buf, int bufstride, const PlanePlan& pl, const double2* __restrict__ roots) {
+template <int NBUF, int MASK, typename C, int BT = 1>
+__device__ __forceinline__ void plane_forward(C* buf, int bufstride, const PlanePlan& pl, const double2* __restrict__ roots) {
 #pragma unroll 1
     for (int d = 0; d < 3; ++d) {
         const AxisPlan& ax = pl.ax[d];
 #pragma unroll 1
         for (int s = 0; s < ax.nst; ++s) {
-            run_stage<true, NBUF, MASK, C>(buf, bufstride, pl.Nk, ax, s, roots);
+            run_stage<true, NBUF, MASK, C, BT>(buf, bufstride, pl.Nk, ax, s, roots);
             __syncthreads();
         }
     }
 }
 
 // Inverse (R -> k, unnormalised sign +1) transform, exact reverse of plane_forward.
-template <int NBUF, int MASK, typename C>
-__device__ void plane_inverse(C* buf, int bufstride, const PlanePlan& pl, const double2* __restrict__ roots) {
+template <int NBUF, int MASK, typename C, int BT = 1>
+__device__ __forceinline__ void plane_inverse(C* buf, int bufstride, const PlanePlan& pl, const double2* __restrict__ roots) {
 #pragma unroll 1
     for (int d = 2; d >= 0; --d) {
         const AxisPlan& ax = pl.ax[d];
 #pragma unroll 1
         for (int s = ax.nst - 1; s >= 0; --s) {
-            run_stage<false, NBUF, MASK, C>(buf, bufstride, pl.Nk, ax, s, roots);
+            run_stage<false, NBUF, MASK, C, BT>(buf, bufstride, pl.Nk, ax, s, roots);
             __syncthreads();
         }
     }

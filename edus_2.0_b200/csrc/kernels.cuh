@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(MAXT) plane_rhs_kernel(
 // inverse transforms run in turn from one buffer; rho(R) survives the first
 // in the CTA's own slot of `scratch` ([gridDim.x][Nk], written and read back
 // by the same thread, so it stays in L2 and needs no fence).
-template <bool COUL, int MASK, int MAXT>
+template <bool COUL, int MASK, int MAXT, int BT = 1>
 __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     const double2* __restrict__ rho, long long batch_stride_in, double2* __restrict__ G_out,
     double2* __restrict__ Hee_out, long long batch_stride_out, const double2* __restrict__ rho0p,
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 const double2* src = rho + (long long)b * batch_stride_in + (long long)p * Nk;
                 for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
                 __syncthreads();
-                plane_forward<1, MASK>(X, 0, pl, roots);
+                plane_forward<1, MASK, double2, BT>(X, 0, pl, roots);
                 const int n = p / nb, m = p - (p / nb) * nb;
                 if (n == m && threadIdx.x == 0) diag0[b * nb + n] = cscale(X[0], inv_nk);
                 __syncthreads();
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 add_model_R(X, hpos, hval, nS, p, P, F, tb, &pl);
                 __syncthreads();
             }
-            plane_inverse<1, MASK>(X, 0, pl, roots);
+            plane_inverse<1, MASK, double2, BT>(X, 0, pl, roots);
             double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
             for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = X[i];
             __syncthreads();  // X is reloaded by the next plane
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 return;
             }
         }
-        plane_forward<1, MASK>(X, 0, pl, roots);
+        plane_forward<1, MASK, double2, BT>(X, 0, pl, roots);
         const StageField F = field[b];
         const int n = p / nb, m = p - (p / nb) * nb;
         if (COUL && n == m && threadIdx.x == 0) diag0[b * nb + n] = cscale(X[0], inv_nk);
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
             X[j] = make_double2(-dot * r.y, dot * r.x);
         }
         __syncthreads();
-        plane_inverse<1, MASK>(X, 0, pl, roots);
+        plane_inverse<1, MASK, double2, BT>(X, 0, pl, roots);
         double2* gdst = G_out + (long long)b * batch_stride_out + (long long)p * Nk;
         if (!bulk) {
             for (int i = threadIdx.x; i < Nk; i += blockDim.x) gdst[i] = X[i];
@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 add_model_R(X, hpos, hval, nS, p, P, F);
                 __syncthreads();
             }
-            plane_inverse<1, MASK>(X, 0, pl, roots);
+            plane_inverse<1, MASK, double2, BT>(X, 0, pl, roots);
             double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
             if (!bulk) {
                 for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = X[i];
@@ -386,21 +386,31 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
 // fits up to 768 threads.  The thread count is chosen per plan so that the
 // butterflies of each stage split into as few, as full, rounds as possible.
 struct PlaneLaunch {
-    int variant;  // 0 generic, 1 radix {8,9}
+    int variant;  // 0 generic (common radices), 1 radix {8,9}, 2 generic with radix 11 or 13
     int threads;
     bool persist;  // persistent single-buffer kernel, two CTAs per SM
 };
+
+// The persistent radix-{8,9} plane kernel: most threads a CTA may have, and
+// butterflies a thread takes at once in each transform stage.
+constexpr int kPersist89Threads = 384;
+constexpr int kPersist89Batch = 1;
 
 inline PlaneLaunch plane_launch(const PlanePlan& pl) {
     bool only89 = true;
     for (int d = 0; d < 3; ++d)
         for (int s = 0; s < pl.ax[d].nst; ++s)
             if (pl.ax[d].r[s] != 8 && pl.ax[d].r[s] != 9) only89 = false;
+    bool wide = false;
+    for (int d = 0; d < 3; ++d)
+        for (int s = 0; s < pl.ax[d].nst; ++s)
+            if (pl.ax[d].r[s] == 11 || pl.ax[d].r[s] == 13) wide = true;
     PlaneLaunch L;
-    L.variant = only89 ? 1 : 0;
+    L.variant = only89 ? 1 : (wide ? 2 : 0);
     // two single-plane CTAs per SM when a plane leaves room for a second one
     L.persist = (size_t)pl.Nk * 16 <= 110 * 1024;
-    const int tmax = L.persist ? (only89 ? 384 : 256) : (only89 ? 768 : 512);
+    const int tmax = L.persist ? (only89 ? kPersist89Threads : 256) : (only89 ? 768 : 512);
+    const int bt = (L.persist && only89) ? kPersist89Batch : 1;
     long best = -1;
     L.threads = tmax;
     for (int T = 128; T <= tmax; T += 32) {
@@ -409,7 +419,7 @@ inline PlaneLaunch plane_launch(const PlanePlan& pl) {
             for (int s = 0; s < pl.ax[d].nst; ++s) {
                 const int r = pl.ax[d].r[s];
                 const long tasks = pl.Nk / r;
-                cost += ((tasks + T - 1) / T) * (long)r;
+                cost += ((tasks + (long)bt * T - 1) / ((long)bt * T)) * (long)r * bt;
             }
         cost = cost * 4 + 3 * ((pl.Nk + T - 1) / T);  // stages (3 transforms) + load/pointwise/store
         if (best < 0 || cost <= best) {
