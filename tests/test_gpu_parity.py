@@ -85,7 +85,7 @@ CASES = [
     ("bulk_ipa_70x60", (70, 60, 1), 2, 2, False),
     # generic odd radices 11 and 13
     ("g11x13", (11, 13, 1), 3, 2, True),
-    ("g3d_13x2x11", (13, 2, 11), 2, 3, False),
+    ("g3d_13x3x11", (13, 3, 11), 2, 3, False),
 ]
 
 
