@@ -6,5 +6,5 @@ that ABI (``edus``) plus the synthetic benchmark workloads (``workloads``).
 The directory name is not a valid Python identifier; load it with
 ``importlib`` (see ``load_package`` in ``__graft_entry__.py``).
 """
-from . import edus, h5, hhg, model, surrogate, workloads  # noqa: F401
+from . import edus, h5, hhg, model, surrogate, sweep, workloads  # noqa: F401
 from .edus import Solver, EdusError, Laser, load_library  # noqa: F401
