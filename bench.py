@@ -519,11 +519,16 @@ def run_reference(args):
 
 
 def run_sweep(args, rank, world, local_rank):
-    """Batched laser sweep: 256 solves of uneven band count and grid (seeded
-    random models, IPA, RK4), grouped by shape into handles with a model per
-    solve, each handle autotuned, all stepped together by edus_sweep_step
-    (chunks of 32 steps captured into one CUDA graph).  Value: solve-steps per
-    second over all solves (wall time around the synchronous sweep call)."""
+    """Batched laser sweep (256 solves of uneven band count and grid: seeded
+    random models, IPA, RK4 dt = 0.005 fs).  The solves are dealt to the ranks
+    by predicted cost (edus_2.0_b200/sweep.py: no data-path collective); on a
+    rank they are grouped by shape into handles with a model per solve, each
+    handle autotuned, and all stepped together by edus_sweep_step in its fused
+    form: per RK stage one persistent launch per plane class and one for the
+    commutators of every solve, chunks of 32 steps captured into a CUDA graph.
+    The per-shape form (every handle on its own stream, one graph) is timed
+    beside it.  Value: solve-steps per second over all solves and ranks (wall
+    time around the synchronous sweep call, max over ranks)."""
     import torch
 
     import __graft_entry__ as ge
@@ -532,14 +537,15 @@ def run_sweep(args, rank, world, local_rank):
     E = pkg.edus
     torch.cuda.set_device(local_rank)
     t_setup = time.perf_counter()
-    specs = pkg.workloads.sweep_specs(args.solves, seed=2024 + rank)
+    specs = pkg.workloads.sweep_specs(args.solves, seed=2024)
+    mine = pkg.sweep.partition(specs, world)[rank]
     cache = os.path.join(tempfile.gettempdir(), f"edus_sweep_{rank}")
     groups = {}
-    for sp in specs:
-        groups.setdefault((sp["nb"], sp["N"]), []).append(sp)
-    handles, tune = [], {}
-    for (nb, N), sps in sorted(groups.items()):
-        models = [pkg.model.Model(pkg.model.parse_input(pkg.workloads.sweep_input(sp, cache))) for sp in sps]
+    for i in mine:
+        groups.setdefault((specs[i]["nb"], specs[i]["N"]), []).append(i)
+    handles, tune, order = [], {}, []
+    for (nb, N), idx in sorted(groups.items()):
+        models = [pkg.model.Model(pkg.model.parse_input(pkg.workloads.sweep_input(specs[i], cache))) for i in idx]
         m0 = models[0]
         s = E.Solver(m0.grid, nb, m0.cfg.dt, batch=len(models), device=local_rank)
         s.upload_model(m0.H0k, m0.xik, m0.A)
@@ -550,32 +556,64 @@ def run_sweep(args, rank, world, local_rank):
             s.set_state(m.rho0k, b)
         tune[f"{nb}x{N}x{N}"] = s.autotune()
         handles.append(s)
+        order.append(idx)
     t_setup = time.perf_counter() - t_setup
-    nsolves = sum(s.batch for s in handles)
-    E.sweep_step(handles, args.warmup, graph=True)
+    nsolves_local = sum(s.batch for s in handles)
+    E.sweep_step(handles, args.warmup, fused=True)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    E.sweep_step(handles, args.steps, graph=True)
-    torch.cuda.synchronize()
-    t_graph = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    E.sweep_step(handles, args.steps, graph=False)
-    torch.cuda.synchronize()
-    t_plain = time.perf_counter() - t0
-    finite = all(np.isfinite(s.get_state(b)).all() for s in handles for b in range(s.batch))
-    value = nsolves * args.steps * world / t_graph
+
+    def timed(**kw):
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        E.sweep_step(handles, args.steps, **kw)
+        torch.cuda.synchronize()
+        t = torch.tensor([time.perf_counter() - t0], device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    with ClockSampler(local_rank) as clocks:
+        t_fused = timed(fused=True)
+    clk = clocks.summary()
+    t_graph = timed(graph=True, fused=False)
+    # observables of every solve, gathered on the host at the end
+    local = {}
+    for s, idx in zip(handles, order):
+        for b, i in enumerate(idx):
+            local[i] = s.population_wannier(b).tolist()
+    merged = pkg.sweep.gather(local, world)
+    finite = bool(len(merged) == len(specs) and all(np.isfinite(v).all() for v in merged.values()))
+    total_solves = len(specs)
+    value = total_solves * args.steps / t_fused
+    step_bytes = sum(pkg.sweep.solve_cost(sp) for sp in specs)  # all ranks, one RK4 step
+    peak, peak_kind = measured_peaks()
+    ach = step_bytes * args.steps / t_fused / 1e9
+    for s in handles:
+        s.close()
     return {
         "metric": "RK4 solve-steps/s, batched laser sweep (256 seeded models, nb in {2,4,8,14,22}, "
                   "N x N grids, N in {24,36,48,72,96}, IPA)",
         "value": round(value, 1), "unit": "solve-steps/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(t_graph / args.steps * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "warmup": args.warmup, "ms_per_step": round(t_fused / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "form": "fused sweep: per RK stage one persistent launch per plane class and one for the commutators "
+                "of every solve, chunks of 32 steps in a CUDA graph",
         "config": {"workload": "sweep: per-solve seeded random TB models, Gaussian pulses (1-3 eV, "
-                               "1e-4..2e-2 a.u.), RK4 dt = 0.005 fs", "solves": nsolves,
-                   "shape_groups": len(handles), "timing": "wall clock around the synchronous sweep call"},
-        "graph_vs_stream_launches": round(t_plain / t_graph, 3),
+                               "1e-4..2e-2 a.u.), RK4 dt = 0.005 fs", "solves": total_solves,
+                   "solves_on_rank0": nsolves_local, "shape_groups_on_rank0": len(handles),
+                   "parallelism": f"solves dealt to {world} rank(s) by predicted cost (LPT)",
+                   "timing": "wall clock around the synchronous sweep call, max over ranks"},
+        "per_shape_streams_graph_s": round(t_graph, 3), "fused_s": round(t_fused, 3),
+        "fused_vs_per_shape": round(t_graph / t_fused, 3),
+        "clocks": clk,
+        "roofline": {"bound": "hbm", "kernel": "whole sweep step", "achieved": round(ach, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+                     "step_bytes": step_bytes, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+                     "bytes_model": "(34 + 4 d_E) S per solve and RK4 step, d_E = 2, S = Nk nb^2 16 B"},
         "autotune": {k: {"plane_threads": v[0], "tensor_commutator": v[1]} for k, v in tune.items()},
-        "setup_s": round(t_setup, 1), "finite": bool(finite),
+        "setup_s": round(t_setup, 1), "finite": finite,
     }
 
 

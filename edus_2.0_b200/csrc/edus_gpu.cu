@@ -18,6 +18,7 @@
 #include "comm_ws.cuh"
 #include "split_kernels.cuh"
 #include "plane3.cuh"
+#include "sweep_kernels.cuh"
 #include <cudaTypedefs.h>
 #include <map>
 #include <mutex>
@@ -1931,6 +1932,202 @@ static int launch_plain_steps(edus_handle* h, int cnt) {
     return EDUS_OK;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Fused sweep (edus_sweep_step with use_graph = 2): per RK stage one
+// persistent plane launch per shared-memory class and one persistent
+// commutator launch for every solve of every handle (csrc/sweep_kernels.cuh).
+struct FusedSweep {
+    int n = 0, C = 0;
+    bool wide = false;
+    PlanePlan* plans = nullptr;
+    SweepPlaneDesc* pdesc = nullptr;
+    StageArgs* args = nullptr;  // [C][4][n]: handle i at step k of a chunk, stage s
+    int* mma = nullptr;         // [n]
+    int4* items = nullptr;      // large planes | small planes | commutator tiles
+    int nl = 0, ns = 0, nc = 0;
+    int* count = nullptr;       // [C][4][3] work counters, zeroed per chunk
+    size_t sm_l = 0, sm_s = 0, sm_c = 0;
+    int thr_c = 256, grid_l = 0, grid_s = 0, grid_c = 0;
+    void release() {
+        cudaFree(plans);
+        cudaFree(pdesc);
+        cudaFree(args);
+        cudaFree(mma);
+        cudaFree(items);
+        cudaFree(count);
+        plans = nullptr;
+        pdesc = nullptr;
+        args = nullptr;
+        mma = nullptr;
+        items = nullptr;
+        count = nullptr;
+    }
+};
+
+// Planes of at most this many bytes leave room for two CTAs on an SM.
+constexpr size_t kSweepSmallPlane = 110 * 1024;
+
+static bool fused_eligible(const edus_handle* h) {
+    return h->d.solver == EDUS_SOLVER_RK && !h->d.coulomb && !h->packed && !h->split && !h->peierls &&
+           h->kg_n == 0 && !h->profiling;
+}
+
+static int fused_setup(edus_handle* const* hs, int n, int C, FusedSweep& f) {
+    edus_handle* h0 = hs[0];
+    f.n = n;
+    f.C = C;
+    std::vector<PlanePlan> plans(n);
+    std::vector<int> mma(n);
+    std::vector<StageArgs> args((size_t)C * 4 * n);
+    struct Item {
+        int4 v;
+        double cost;
+    };
+    std::vector<Item> large, small, comm;
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h0->d.device);
+    for (int i = 0; i < n; ++i) {
+        edus_handle* h = hs[i];
+        plans[i] = h->plan;
+        mma[i] = h->comm_mma ? 1 : 0;
+        if (plane_launch(h->plan).variant == 2) f.wide = true;
+        const double dt = h->d.dt;
+        const double c0[4] = {dt / 2., dt / 2., dt, dt / 6.};
+        const double c1[4] = {dt / 6., dt / 3., dt / 3., 0.};
+        for (int k = 0; k < C; ++k)
+            for (int st = 0; st < 4; ++st) {
+                StageArgs a = base_args(h);
+                a.y = h->y;
+                a.aux = h->aux;
+                a.acc = h->acc;
+                a.rho = st == 0 ? h->y : h->aux;
+                a.field = h->field + ((size_t)k * 4 + st) * h->B;
+                a.c[0] = c0[st];
+                a.c[1] = c1[st];
+                args[((size_t)k * 4 + st) * n + i] = a;
+            }
+        const size_t plane_bytes = (size_t)h->Nk * sizeof(double2);
+        auto& dst = plane_bytes > kSweepSmallPlane ? large : small;
+        (plane_bytes > kSweepSmallPlane ? f.sm_l : f.sm_s) =
+            std::max(plane_bytes > kSweepSmallPlane ? f.sm_l : f.sm_s, plane_bytes);
+        const double pcost = (double)h->Nk * std::log2((double)std::max(h->Nk, 2));
+        for (int b = 0; b < h->B; ++b)
+            for (int p = 0; p < h->P; ++p) dst.push_back({make_int4(i, b, p, 0), pcost});
+        const int ntile = (h->Nk + h->TK - 1) / h->TK;
+        const double ccost = (double)h->TK * h->nb * h->nb * h->nb;
+        for (int b = 0; b < h->B; ++b)
+            for (int t = 0; t < ntile; ++t) comm.push_back({make_int4(i, b, t, 0), ccost});
+        f.sm_c = std::max(f.sm_c, (size_t)h->smem_comm);
+        f.thr_c = std::max(f.thr_c, h->comm_threads);
+    }
+    auto by_cost = [](const Item& x, const Item& y) { return x.cost > y.cost; };
+    std::stable_sort(large.begin(), large.end(), by_cost);
+    std::stable_sort(small.begin(), small.end(), by_cost);
+    std::stable_sort(comm.begin(), comm.end(), by_cost);
+    f.nl = (int)large.size();
+    f.ns = (int)small.size();
+    f.nc = (int)comm.size();
+    std::vector<int4> items;
+    items.reserve(large.size() + small.size() + comm.size());
+    for (auto& x : large) items.push_back(x.v);
+    for (auto& x : small) items.push_back(x.v);
+    for (auto& x : comm) items.push_back(x.v);
+    auto alloc_copy = [&](void** p, const void* src, size_t bytes) -> int {
+        if (cudaMalloc(p, bytes) != cudaSuccess) return fail(h0, EDUS_ERR_CUDA, "fused sweep: cudaMalloc failed");
+        if (src && cudaMemcpy(*p, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(h0, EDUS_ERR_CUDA, "fused sweep: upload failed");
+        return EDUS_OK;
+    };
+    int rc;
+    if ((rc = alloc_copy((void**)&f.plans, plans.data(), n * sizeof(PlanePlan)))) return rc;
+    std::vector<SweepPlaneDesc> pd(n);
+    for (int i = 0; i < n; ++i) {
+        edus_handle* h = hs[i];
+        pd[i] = SweepPlaneDesc{f.plans + i, h->roots, h->rpos, h->G, (long long)h->S, h->Nk, 1.0 / h->Nk};
+    }
+    if ((rc = alloc_copy((void**)&f.pdesc, pd.data(), n * sizeof(SweepPlaneDesc)))) return rc;
+    if ((rc = alloc_copy((void**)&f.args, args.data(), args.size() * sizeof(StageArgs)))) return rc;
+    if ((rc = alloc_copy((void**)&f.mma, mma.data(), n * sizeof(int)))) return rc;
+    if ((rc = alloc_copy((void**)&f.items, items.data(), std::max<size_t>(items.size(), 1) * sizeof(int4)))) return rc;
+    if ((rc = alloc_copy((void**)&f.count, nullptr, (size_t)C * 4 * 3 * sizeof(int)))) return rc;
+    // kernel attributes (process-wide: the device maximum, as for every kernel here)
+    const int optin = device_smem_optin(h0->d.device);
+    if ((size_t)optin < std::max(f.sm_l, std::max(f.sm_s, f.sm_c)))
+        return fail(h0, EDUS_ERR_UNSUPPORTED, "fused sweep: a plane exceeds shared memory");
+    cudaFuncSetAttribute(sweep_plane_kernel<kRadixCommon, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncSetAttribute(sweep_plane_kernel<kRadixCommon, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncSetAttribute(sweep_plane_kernel<kRadixAll, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncSetAttribute(sweep_plane_kernel<kRadixAll, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+#define EDUS_SWEEP_ATTR(M)                                                                                    \
+    cudaFuncSetAttribute(sweep_comm_kernel<M, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin); \
+    cudaFuncSetAttribute(sweep_comm_kernel<M, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    EDUS_SWEEP_ATTR(MODE_RK1)
+    EDUS_SWEEP_ATTR(MODE_RK2)
+    EDUS_SWEEP_ATTR(MODE_RK3)
+    EDUS_SWEEP_ATTR(MODE_RK4)
+#undef EDUS_SWEEP_ATTR
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_plane_kernel<kRadixCommon, 256>, 256, f.sm_s);
+    f.grid_s = nsm * std::max(per, 1);
+    f.grid_l = nsm;
+    per = 0;
+    if (f.thr_c <= 256)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_comm_kernel<MODE_RK1, 256>, 256, f.sm_c);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_comm_kernel<MODE_RK1, 512>, 512, f.sm_c);
+    f.grid_c = nsm * std::max(per, 1);
+    f.thr_c = f.thr_c <= 256 ? 256 : 512;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h0, EDUS_ERR_CUDA, std::string("fused sweep set-up: ") + cudaGetErrorString(e));
+    return EDUS_OK;
+}
+
+template <int MODE>
+static void fused_comm_launch(const FusedSweep& f, const StageArgs* args, int* cnt, cudaStream_t st) {
+    const int4* it = f.items + f.nl + f.ns;
+    if (f.thr_c == 256)
+        sweep_comm_kernel<MODE, 256><<<f.grid_c, 256, f.sm_c, st>>>(args, f.mma, it, f.nc, cnt);
+    else
+        sweep_comm_kernel<MODE, 512><<<f.grid_c, 512, f.sm_c, st>>>(args, f.mma, it, f.nc, cnt);
+}
+
+// `cnt` RK4 steps of every handle of the sweep, all on stream st.
+static int fused_launch_steps(edus_handle* const* hs, const FusedSweep& f, int cnt, cudaStream_t st) {
+    edus_handle* h0 = hs[0];
+    if (cudaMemsetAsync(f.count, 0, (size_t)f.C * 4 * 3 * sizeof(int), st) != cudaSuccess)
+        return fail(h0, EDUS_ERR_CUDA, "fused sweep: counter reset failed");
+    for (int k = 0; k < cnt; ++k) {
+        for (int s = 0; s < 4; ++s) {
+            const StageArgs* a = f.args + ((size_t)k * 4 + s) * f.n;
+            int* c = f.count + ((size_t)k * 4 + s) * 3;
+            if (f.nl) {
+                if (f.wide) sweep_plane_kernel<kRadixAll, 512><<<f.grid_l, 512, f.sm_l, st>>>(f.pdesc, a, f.items, f.nl, c);
+                else sweep_plane_kernel<kRadixCommon, 512><<<f.grid_l, 512, f.sm_l, st>>>(f.pdesc, a, f.items, f.nl, c);
+            }
+            if (f.ns) {
+                const int4* it = f.items + f.nl;
+                if (f.wide) sweep_plane_kernel<kRadixAll, 256><<<f.grid_s, 256, f.sm_s, st>>>(f.pdesc, a, it, f.ns, c + 1);
+                else sweep_plane_kernel<kRadixCommon, 256><<<f.grid_s, 256, f.sm_s, st>>>(f.pdesc, a, it, f.ns, c + 1);
+            }
+            switch (s) {
+                case 0: fused_comm_launch<MODE_RK1>(f, a, c + 2, st); break;
+                case 1: fused_comm_launch<MODE_RK2>(f, a, c + 2, st); break;
+                case 2: fused_comm_launch<MODE_RK3>(f, a, c + 2, st); break;
+                default: fused_comm_launch<MODE_RK4>(f, a, c + 2, st); break;
+            }
+            h0->launches += (f.nl ? 1 : 0) + (f.ns ? 1 : 0) + 1;
+        }
+        for (int i = 0; i < f.n; ++i) hs[i]->t += hs[i]->d.dt;
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h0, EDUS_ERR_CUDA, std::string("fused sweep launch: ") + cudaGetErrorString(e));
+    return EDUS_OK;
+}
+
+extern "C" {
+
 int edus_step(edus_handle* h, int n) {
     if (!h || n < 0) return EDUS_ERR_ARG;
     if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "edus_upload_model must be called first");
@@ -2000,6 +2197,7 @@ int edus_sweep_step(edus_handle* const* hs, int n, int steps, int use_graph) {
         if (!hs[i]) return EDUS_ERR_ARG;
     edus_handle* h0 = hs[0];
     bool graph = use_graph != 0;
+    const bool fused = use_graph == 2;
     for (int i = 0; i < n; ++i) {
         edus_handle* h = hs[i];
         if (h->d.device != h0->d.device) return fail(h0, EDUS_ERR_ARG, "a sweep's handles share one device");
@@ -2009,6 +2207,10 @@ int edus_sweep_step(edus_handle* const* hs, int n, int steps, int use_graph) {
         for (int j = 0; j < i; ++j)
             if (hs[j] == h) return fail(h, EDUS_ERR_ARG, "a handle appears twice in the sweep");
         if (h->d.solver != EDUS_SOLVER_RK || h->profiling) graph = false;
+        if (fused && !fused_eligible(h))
+            return fail(h, EDUS_ERR_UNSUPPORTED,
+                        "the fused sweep steps RK4 independent-particle handles (no HSEX, Peierls, k-space gradient "
+                        "or profiling)");
     }
     if (steps == 0) return EDUS_OK;
     CU(h0, cudaSetDevice(h0->d.device));
@@ -2017,9 +2219,11 @@ int edus_sweep_step(edus_handle* const* hs, int n, int steps, int use_graph) {
     cudaEvent_t fork = nullptr;
     std::vector<cudaEvent_t> join(n, nullptr);
     cudaGraphExec_t exec = nullptr;
+    FusedSweep fs;
     int rc = EDUS_OK;
     auto cleanup = [&]() {
         if (s0) cudaStreamSynchronize(s0);
+        fs.release();
         if (exec) cudaGraphExecDestroy(exec);
         for (auto& e : join)
             if (e) cudaEventDestroy(e);
@@ -2043,12 +2247,18 @@ int edus_sweep_step(edus_handle* const* hs, int n, int steps, int use_graph) {
             return fail(h0, EDUS_ERR_CUDA, std::string("sweep set-up: ") + cudaGetErrorString(pend));
         }
     }
+    if (fused && (rc = fused_setup(hs, n, C, fs))) {
+        cleanup();
+        return rc;
+    }
     // every handle's launches of `cnt` steps, forked from and joined into s0
+    // (fused: the persistent launches of every handle, on s0)
     auto launch_all = [&](int cnt) -> int {
         {
             const cudaError_t pend = cudaGetLastError();
             if (pend != cudaSuccess) return fail(h0, EDUS_ERR_CUDA, std::string("sweep, before launches: ") + cudaGetErrorString(pend));
         }
+        if (fused) return fused_launch_steps(hs, fs, cnt, s0);
         if (cudaEventRecord(fork, s0) != cudaSuccess) return fail(h0, EDUS_ERR_CUDA, "cudaEventRecord failed");
         for (int i = 0; i < n; ++i) {
             edus_handle* h = hs[i];
@@ -2113,8 +2323,9 @@ int edus_sweep_step(edus_handle* const* hs, int n, int steps, int use_graph) {
             }
             for (int i = 0; i < n; ++i) {
                 for (int k = 0; k < C; ++k) hs[i]->t += hs[i]->d.dt;  // as the launches would
-                hs[i]->launches += 8LL * C;
+                if (!fused) hs[i]->launches += 8LL * C;
             }
+            if (fused) h0->launches += (unsigned long long)C * 4 * ((fs.nl ? 1 : 0) + (fs.ns ? 1 : 0) + 1);
         } else {
             rc = launch_all(cnt);
         }

@@ -602,9 +602,11 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs& a, const double2
     }
 }
 
+// One (k tile, solve) of the CUDA-core commutator: the body of
+// commutator_kernel, also run by the sweep's persistent commutator kernel.
+// Any blockDim with TK * tiles <= 2 * blockDim works.
 template <int MODE, bool COUL, bool FH = false>
-__global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
-    extern __shared__ double2 sm[];
+__device__ __forceinline__ void commutator_tile(const StageArgs& a, int b, int tile, double2* sm) {
     const int nb = a.nb, TK = a.TK;
     const int nbp = (nb + 1) & ~1, ld = nbp + 1;
     const int tile_stride = nbp * ld;
@@ -612,8 +614,7 @@ __global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
     double2* Rs = sm + TK * tile_stride;     // [TK][nbp][ld]
     double2* hh = Rs + TK * tile_stride;     // [nb] Hartree shift
     double2* Cs = sm;                        // [P][TK], over Hs once the products are done
-    const int b = blockIdx.y;
-    const int k0 = blockIdx.x * TK;
+    const int k0 = tile * TK;
     const StageField F = a.field[b];
     if (COUL) {
         for (int n = threadIdx.x; n < nb; n += blockDim.x) {
@@ -698,6 +699,12 @@ __global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
     stage_epilogue<MODE>(a, Cs, b, k0);
 }
 
+template <int MODE, bool COUL, bool FH = false>
+__global__ void __launch_bounds__(512) commutator_kernel(StageArgs a) {
+    extern __shared__ double2 sm[];
+    commutator_tile<MODE, COUL, FH>(a, blockIdx.y, blockIdx.x, sm);
+}
+
 // ---------------------------------------------------------------------------
 // Tensor-core commutator for nb >= 12: the same contract as commutator_kernel,
 // with C = H rho - rho H done by FP64 warp MMAs (mma.sync m8n8k4, 8x8 output
@@ -758,9 +765,11 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
+// One (k tile, solve) of the FP64 tensor-core commutator: the body of
+// commutator_mma_kernel, also run by the sweep's persistent commutator kernel.
+// Warps past the first 8 take no product tiles (kk >= TK below).
 template <int MODE, bool COUL, bool FH = false>
-__global__ void __launch_bounds__(256, 2) commutator_mma_kernel(StageArgs a) {
-    extern __shared__ double smd[];
+__device__ __forceinline__ void commutator_mma_tile(const StageArgs& a, int b, int tile, double* smd) {
     const int nb = a.nb, Nk = a.Nk;
     const MmaGeom g = mma_geometry(nb);
     const int TK = g.TK, nbp = g.nbp, pitch = g.pitch;
@@ -768,8 +777,7 @@ __global__ void __launch_bounds__(256, 2) commutator_mma_kernel(StageArgs a) {
     double* tiles = smd;          // [TK][4][nbp][pitch]: Hr, Hi, Rr, Ri
     double2* hh = (double2*)(smd + (size_t)TK * 4 * mat);
     double2* Cs = (double2*)smd;  // [P][TK] after the products
-    const int b = blockIdx.y;
-    const int k0 = blockIdx.x * TK;
+    const int k0 = tile * TK;
     const StageField F = a.field[b];
     for (int i = threadIdx.x; i < TK * 4 * mat; i += blockDim.x) tiles[i] = 0.0;
     if (COUL) {
@@ -852,6 +860,12 @@ __global__ void __launch_bounds__(256, 2) commutator_mma_kernel(StageArgs a) {
     }
     __syncthreads();
     stage_epilogue<MODE>(a, Cs, b, k0);
+}
+
+template <int MODE, bool COUL, bool FH = false>
+__global__ void __launch_bounds__(256, 2) commutator_mma_kernel(StageArgs a) {
+    extern __shared__ double smd[];
+    commutator_mma_tile<MODE, COUL, FH>(a, blockIdx.y, blockIdx.x, smd);
 }
 
 // ---------------------------------------------------------------------------

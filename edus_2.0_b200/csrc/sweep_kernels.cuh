@@ -1,0 +1,107 @@
+// Persistent kernels that advance a whole sweep of uneven solves (different
+// band counts and k grids, independent-particle RHS, FP64, RK4) with one
+// launch per RK stage for the plane transforms of every solve (per shared
+// memory class: planes that leave room for two CTAs on an SM, and larger
+// ones) and one launch for the commutators and stage updates of every solve.
+//
+// Work items are (shape handle, solve, plane) and (shape handle, solve, k
+// tile), ordered by decreasing cost on the host; a CTA takes the next item of
+// its launch from an atomic counter (largest first onto whichever CTA is
+// free), so the solves of small shapes fill the SMs that the large ones leave.
+// Each item runs the same device code as the shape's own kernels
+// (plane_forward / plane_inverse with the gradient of kGradient_definitions.hpp:34-40;
+// commutator_tile / commutator_mma_tile with the RK stage epilogue of
+// DESolver.hpp:154-187), so a solve's result does not depend on the launch it
+// ran in.
+#pragma once
+#include "kernels.cuh"
+
+namespace edus {
+
+// What a plane item needs from its shape beyond the stage arguments.
+struct SweepPlaneDesc {
+    const PlanePlan* plan;  // device copy of the shape's plan
+    const double2* roots;
+    const double* rpos;
+    double2* G;             // gradient term out, [B][P][Nk]
+    long long S;            // P * Nk (solve stride)
+    int Nk;
+    double inv_nk;
+};
+
+// The next item of this launch for the whole CTA (from `counter`, which the
+// host zeroes before the launch).
+__device__ __forceinline__ int sweep_fetch(int* counter, int* slot) {
+    __syncthreads();  // every thread is done with the previous item (and its shared memory)
+    if (threadIdx.x == 0) *slot = atomicAdd(counter, 1);
+    __syncthreads();
+    return *slot;
+}
+
+// Plane items {shape, solve, plane}: rho_R = FFT(rho_k)/Nk, G_R = i (R.E) rho_R,
+// G_k = FFT^-1(G_R).  args[shape] are the shape's stage arguments (stage input
+// rho, field table of the stage).
+template <int MASK, int MAXT>
+__global__ void __launch_bounds__(MAXT) sweep_plane_kernel(const SweepPlaneDesc* __restrict__ descs,
+                                                           const StageArgs* __restrict__ args,
+                                                           const int4* __restrict__ items, int nitems, int* counter) {
+    extern __shared__ double2 X[];
+    __shared__ int s_item;
+    for (;;) {
+        const int w = sweep_fetch(counter, &s_item);
+        if (w >= nitems) break;
+        const int4 it = items[w];
+        const SweepPlaneDesc& d = descs[it.x];
+        const StageArgs& a = args[it.x];
+        const PlanePlan& pl = *d.plan;
+        const int Nk = d.Nk;
+        const long long off = (long long)it.y * d.S + (long long)it.z * Nk;
+        const double2* src = a.rho + off;
+        for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
+        __syncthreads();
+        plane_forward<1, MASK>(X, 0, pl, d.roots);
+        const StageField F = a.field[it.y];
+        const int n1 = pl.ax[1].n, n2 = pl.ax[2].n;
+        const double* rp0 = d.rpos + pl.ax[0].rposoff;
+        const double* rp1 = d.rpos + pl.ax[1].rposoff;
+        const double* rp2 = d.rpos + pl.ax[2].rposoff;
+        for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
+            const int t = fdiv(j, pl.fd_n2);
+            const int q2 = j - t * n2;
+            const int q0 = fdiv(t, pl.fd_n1);
+            const int q1 = t - q0 * n1;
+            const double dot = F.g[0] * __ldg(&rp0[q0]) + F.g[1] * __ldg(&rp1[q1]) + F.g[2] * __ldg(&rp2[q2]);
+            const double2 r = cscale(X[j], d.inv_nk);
+            X[j] = make_double2(-dot * r.y, dot * r.x);
+        }
+        __syncthreads();
+        plane_inverse<1, MASK>(X, 0, pl, d.roots);
+        double2* dst = d.G + off;
+        for (int i = threadIdx.x; i < Nk; i += blockDim.x) dst[i] = X[i];
+    }
+}
+
+// Commutator items {shape, solve, k tile}: f = G - i[H0 + E.xi, rho] and the
+// RK stage update of the shape's arrays, on the FP64 tensor cores where the
+// shape's handle uses them (mma[shape] != 0), on CUDA cores otherwise.  MAXT
+// is at least every shape's commutator thread count (256 for fewer than 46
+// bands).
+template <int MODE, int MAXT>
+__global__ void __launch_bounds__(MAXT) sweep_comm_kernel(const StageArgs* __restrict__ args,
+                                                         const int* __restrict__ mma,
+                                                         const int4* __restrict__ items, int nitems, int* counter) {
+    extern __shared__ double2 sm[];
+    __shared__ int s_item;
+    for (;;) {
+        const int w = sweep_fetch(counter, &s_item);
+        if (w >= nitems) break;
+        const int4 it = items[w];
+        const StageArgs& a = args[it.x];
+        if (mma[it.x])
+            commutator_mma_tile<MODE, false>(a, it.y, it.z, (double*)sm);
+        else
+            commutator_tile<MODE, false>(a, it.y, it.z, sm);
+    }
+}
+
+}  // namespace edus

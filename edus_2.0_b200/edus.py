@@ -380,16 +380,18 @@ class Solver:
         return v.value
 
 
-def sweep_step(solvers, steps, graph=True):
+def sweep_step(solvers, steps, graph=True, fused=False):
     """Advance several Solvers (one device, FP64 form) by `steps` steps
     together (edus_sweep_step): each on its own stream, chunks of RK4 steps
-    captured into one CUDA graph when `graph`."""
+    captured into one CUDA graph when `graph`; with `fused`, one persistent
+    launch per RK stage for the planes and one for the commutators of every
+    solve (independent-particle RK4 handles), captured the same way."""
     if not solvers:
         return
     L = solvers[0]._L
     arr = (ctypes.c_void_p * len(solvers))(*[s._h.value if hasattr(s._h, "value") else s._h for s in solvers])
     rc = L.edus_sweep_step(ctypes.cast(arr, ctypes.POINTER(ctypes.c_void_p)), len(solvers), int(steps),
-                           1 if graph else 0)
+                           2 if fused else (1 if graph else 0))
     if rc:
         msgs = "; ".join(L.edus_last_error(s._h).decode() for s in solvers if L.edus_last_error(s._h))
         raise EdusError(rc, msgs)

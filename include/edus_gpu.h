@@ -172,12 +172,23 @@ int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k);
  * Asynchronous: returns once the work is queued. */
 int edus_step(edus_handle* h, int n);
 
-/* Advance n handles (one device, FP64 form) by `steps` steps together: every
- * handle's kernels run on its own stream, forked from and joined into one
- * sweep stream, so solves of different grids and band counts share the GPU.
- * With use_graph != 0 and RK4 handles, each chunk of 32 steps of all handles
- * is captured once into one CUDA graph and replayed (the field tables are
- * refreshed between replays).  Synchronous.  No reference counterpart. */
+/* Advance n handles (one device, FP64 form) by `steps` steps together.
+ *   use_graph = 0: every handle's kernels run on its own stream, forked from
+ *                  and joined into one sweep stream, so solves of different
+ *                  grids and band counts share the GPU;
+ *   use_graph = 1: the same, and with RK4 handles each chunk of 32 steps of all
+ *                  handles is captured once into one CUDA graph and replayed
+ *                  (the field tables are refreshed between replays);
+ *   use_graph = 2: one persistent launch per RK stage for the plane transforms
+ *                  of every solve of every handle (one per shared-memory class:
+ *                  planes up to 110 KB, larger planes) and one for all their
+ *                  commutators and stage updates; work items (handle, solve,
+ *                  plane or k tile) are taken largest first from a counter;
+ *                  chunks captured into a CUDA graph.  RK4, independent
+ *                  particles, R-space gradient, length gauge (else
+ *                  EDUS_ERR_UNSUPPORTED).  A solve's result equals stepping
+ *                  its handle alone.
+ * Synchronous.  No reference counterpart. */
 int edus_sweep_step(edus_handle* const* hs, int n, int steps, int use_graph);
 
 /* Time the launch variants on the handle's own data and keep the fastest:
