@@ -1935,34 +1935,50 @@ static int launch_plain_steps(edus_handle* h, int cnt) {
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// Fused sweep (edus_sweep_step with use_graph = 2): per RK stage one
-// persistent plane launch per shared-memory class and one persistent
-// commutator launch for every solve of every handle (csrc/sweep_kernels.cuh).
+// Fused sweep (edus_sweep_step with use_graph = 2).  The handles form two
+// groups by plane size: planes above 110 KB (one CTA per SM) and the rest
+// (two per SM).  Each group advances on its own stream with, per RK stage,
+// one persistent plane launch over every plane of its solves and one
+// persistent commutator launch per commutator kind (FP64 tensor cores, CUDA
+// cores) over every k tile of its solves (csrc/sweep_kernels.cuh); the two
+// groups are independent, so one group's transforms overlap the other's
+// commutators.
+struct FusedGroup {
+    int np = 0, ncm = 0, ncc = 0;   // plane items, tensor-core and CUDA-core tiles
+    int off = 0;                    // first item in FusedSweep::items
+    size_t sm_p = 0, sm_cm = 0, sm_cc = 0;
+    int thr_p = 256, grid_p = 0, grid_cm = 0, grid_cc = 0;
+};
+
 struct FusedSweep {
     int n = 0, C = 0;
     bool wide = false;
     PlanePlan* plans = nullptr;
     SweepPlaneDesc* pdesc = nullptr;
     StageArgs* args = nullptr;  // [C][4][n]: handle i at step k of a chunk, stage s
-    int* mma = nullptr;         // [n]
-    int4* items = nullptr;      // large planes | small planes | commutator tiles
-    int nl = 0, ns = 0, nc = 0;
-    int* count = nullptr;       // [C][4][3] work counters, zeroed per chunk
-    size_t sm_l = 0, sm_s = 0, sm_c = 0;
-    int thr_c = 256, grid_l = 0, grid_s = 0, grid_c = 0;
+    int4* items = nullptr;      // per group: planes | tensor-core tiles | CUDA-core tiles
+    FusedGroup g[2];            // 0: planes above 110 KB, 1: the others
+    int thr_c = 256;
+    bool tiles5 = true;         // every tensor-core shape needs at most 5 tiles per warp
+    int* count = nullptr;       // [C][4][2][3] work counters, zeroed per chunk
+    cudaStream_t s1 = nullptr;  // the second group's stream
+    cudaEvent_t fork = nullptr, join = nullptr;
     void release() {
         cudaFree(plans);
         cudaFree(pdesc);
         cudaFree(args);
-        cudaFree(mma);
         cudaFree(items);
         cudaFree(count);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (s1) cudaStreamDestroy(s1);
         plans = nullptr;
         pdesc = nullptr;
         args = nullptr;
-        mma = nullptr;
         items = nullptr;
         count = nullptr;
+        fork = join = nullptr;
+        s1 = nullptr;
     }
 };
 
@@ -1979,19 +1995,17 @@ static int fused_setup(edus_handle* const* hs, int n, int C, FusedSweep& f) {
     f.n = n;
     f.C = C;
     std::vector<PlanePlan> plans(n);
-    std::vector<int> mma(n);
     std::vector<StageArgs> args((size_t)C * 4 * n);
     struct Item {
         int4 v;
         double cost;
     };
-    std::vector<Item> large, small, comm;
+    std::vector<Item> planes[2], comm_m[2], comm_c[2];
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h0->d.device);
     for (int i = 0; i < n; ++i) {
         edus_handle* h = hs[i];
         plans[i] = h->plan;
-        mma[i] = h->comm_mma ? 1 : 0;
         if (plane_launch(h->plan).variant == 2) f.wide = true;
         const double dt = h->d.dt;
         const double c0[4] = {dt / 2., dt / 2., dt, dt / 6.};
@@ -2009,31 +2023,39 @@ static int fused_setup(edus_handle* const* hs, int n, int C, FusedSweep& f) {
                 args[((size_t)k * 4 + st) * n + i] = a;
             }
         const size_t plane_bytes = (size_t)h->Nk * sizeof(double2);
-        auto& dst = plane_bytes > kSweepSmallPlane ? large : small;
-        (plane_bytes > kSweepSmallPlane ? f.sm_l : f.sm_s) =
-            std::max(plane_bytes > kSweepSmallPlane ? f.sm_l : f.sm_s, plane_bytes);
+        const int gi = plane_bytes > kSweepSmallPlane ? 0 : 1;
+        FusedGroup& G = f.g[gi];
+        G.sm_p = std::max(G.sm_p, plane_bytes);
         const double pcost = (double)h->Nk * std::log2((double)std::max(h->Nk, 2));
         for (int b = 0; b < h->B; ++b)
-            for (int p = 0; p < h->P; ++p) dst.push_back({make_int4(i, b, p, 0), pcost});
+            for (int p = 0; p < h->P; ++p) planes[gi].push_back({make_int4(i, b, p, 0), pcost});
         const int ntile = (h->Nk + h->TK - 1) / h->TK;
         const double ccost = (double)h->TK * h->nb * h->nb * h->nb;
+        auto& cdst = h->comm_mma ? comm_m[gi] : comm_c[gi];
         for (int b = 0; b < h->B; ++b)
-            for (int t = 0; t < ntile; ++t) comm.push_back({make_int4(i, b, t, 0), ccost});
-        f.sm_c = std::max(f.sm_c, (size_t)h->smem_comm);
+            for (int t = 0; t < ntile; ++t) cdst.push_back({make_int4(i, b, t, 0), ccost});
+        if (h->comm_mma) {
+            const MmaGeom mg = mma_geometry(h->nb);
+            if ((mg.tiles * mg.tiles + mg.warps_per_k - 1) / mg.warps_per_k > 5) f.tiles5 = false;
+        }
+        if (h->comm_mma) G.sm_cm = std::max(G.sm_cm, (size_t)h->smem_comm);
+        else G.sm_cc = std::max(G.sm_cc, (size_t)h->smem_comm);
         f.thr_c = std::max(f.thr_c, h->comm_threads);
     }
+    f.thr_c = f.thr_c <= 256 ? 256 : 512;
     auto by_cost = [](const Item& x, const Item& y) { return x.cost > y.cost; };
-    std::stable_sort(large.begin(), large.end(), by_cost);
-    std::stable_sort(small.begin(), small.end(), by_cost);
-    std::stable_sort(comm.begin(), comm.end(), by_cost);
-    f.nl = (int)large.size();
-    f.ns = (int)small.size();
-    f.nc = (int)comm.size();
     std::vector<int4> items;
-    items.reserve(large.size() + small.size() + comm.size());
-    for (auto& x : large) items.push_back(x.v);
-    for (auto& x : small) items.push_back(x.v);
-    for (auto& x : comm) items.push_back(x.v);
+    for (int gi = 0; gi < 2; ++gi) {
+        for (auto* v : {&planes[gi], &comm_m[gi], &comm_c[gi]}) std::stable_sort(v->begin(), v->end(), by_cost);
+        FusedGroup& G = f.g[gi];
+        G.off = (int)items.size();
+        G.np = (int)planes[gi].size();
+        G.ncm = (int)comm_m[gi].size();
+        G.ncc = (int)comm_c[gi].size();
+        G.thr_p = gi == 0 ? 512 : 256;
+        for (auto* v : {&planes[gi], &comm_m[gi], &comm_c[gi]})
+            for (auto& x : *v) items.push_back(x.v);
+    }
     auto alloc_copy = [&](void** p, const void* src, size_t bytes) -> int {
         if (cudaMalloc(p, bytes) != cudaSuccess) return fail(h0, EDUS_ERR_CUDA, "fused sweep: cudaMalloc failed");
         if (src && cudaMemcpy(*p, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
@@ -2049,78 +2071,128 @@ static int fused_setup(edus_handle* const* hs, int n, int C, FusedSweep& f) {
     }
     if ((rc = alloc_copy((void**)&f.pdesc, pd.data(), n * sizeof(SweepPlaneDesc)))) return rc;
     if ((rc = alloc_copy((void**)&f.args, args.data(), args.size() * sizeof(StageArgs)))) return rc;
-    if ((rc = alloc_copy((void**)&f.mma, mma.data(), n * sizeof(int)))) return rc;
     if ((rc = alloc_copy((void**)&f.items, items.data(), std::max<size_t>(items.size(), 1) * sizeof(int4)))) return rc;
-    if ((rc = alloc_copy((void**)&f.count, nullptr, (size_t)C * 4 * 3 * sizeof(int)))) return rc;
-    // kernel attributes (process-wide: the device maximum, as for every kernel here)
+    if ((rc = alloc_copy((void**)&f.count, nullptr, (size_t)C * 4 * 2 * 3 * sizeof(int)))) return rc;
+    if (cudaStreamCreateWithFlags(&f.s1, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&f.join, cudaEventDisableTiming) != cudaSuccess)
+        return fail(h0, EDUS_ERR_CUDA, "fused sweep: stream/event creation failed");
+    // kernel attributes (process-wide: the device maximum less the kernel's
+    // static shared memory, as for every kernel here)
     const int optin = device_smem_optin(h0->d.device);
-    if ((size_t)optin < std::max(f.sm_l, std::max(f.sm_s, f.sm_c)))
-        return fail(h0, EDUS_ERR_UNSUPPORTED, "fused sweep: a plane exceeds shared memory");
-    cudaFuncSetAttribute(sweep_plane_kernel<kRadixCommon, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    cudaFuncSetAttribute(sweep_plane_kernel<kRadixCommon, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    cudaFuncSetAttribute(sweep_plane_kernel<kRadixAll, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    cudaFuncSetAttribute(sweep_plane_kernel<kRadixAll, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-#define EDUS_SWEEP_ATTR(M)                                                                                    \
-    cudaFuncSetAttribute(sweep_comm_kernel<M, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin); \
-    cudaFuncSetAttribute(sweep_comm_kernel<M, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    for (const FusedGroup& G : f.g)
+        if ((size_t)optin < std::max(G.sm_p, std::max(G.sm_cm, G.sm_cc)) + 64)
+            return fail(h0, EDUS_ERR_UNSUPPORTED, "fused sweep: a plane exceeds shared memory");
+    auto dyn_max = [optin](auto kernel) {
+        cudaFuncAttributes fa{};
+        cudaFuncGetAttributes(&fa, kernel);
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    };
+    dyn_max(sweep_plane_kernel<kRadixCommon, 256>);
+    dyn_max(sweep_plane_kernel<kRadixCommon, 512>);
+    dyn_max(sweep_plane_kernel<kRadixAll, 256>);
+    dyn_max(sweep_plane_kernel<kRadixAll, 512>);
+#define EDUS_SWEEP_ATTR(M)                             \
+    dyn_max(sweep_comm_kernel<M, 256, true, 5>);       \
+    dyn_max(sweep_comm_kernel<M, 256, true, 8>);       \
+    dyn_max(sweep_comm_kernel<M, 256, false>);         \
+    dyn_max(sweep_comm_kernel<M, 512, true, 5>);       \
+    dyn_max(sweep_comm_kernel<M, 512, true, 8>);       \
+    dyn_max(sweep_comm_kernel<M, 512, false>);
     EDUS_SWEEP_ATTR(MODE_RK1)
     EDUS_SWEEP_ATTR(MODE_RK2)
     EDUS_SWEEP_ATTR(MODE_RK3)
     EDUS_SWEEP_ATTR(MODE_RK4)
 #undef EDUS_SWEEP_ATTR
-    int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_plane_kernel<kRadixCommon, 256>, 256, f.sm_s);
-    f.grid_s = nsm * std::max(per, 1);
-    f.grid_l = nsm;
-    per = 0;
-    if (f.thr_c <= 256)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_comm_kernel<MODE_RK1, 256>, 256, f.sm_c);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_comm_kernel<MODE_RK1, 512>, 512, f.sm_c);
-    f.grid_c = nsm * std::max(per, 1);
-    f.thr_c = f.thr_c <= 256 ? 256 : 512;
+    // grids: as many CTAs as fit on the device at once
+    for (FusedGroup& G : f.g) {
+        int per = 0;
+        if (G.thr_p == 512) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_plane_kernel<kRadixCommon, 512>, 512, G.sm_p);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_plane_kernel<kRadixCommon, 256>, 256, G.sm_p);
+        G.grid_p = nsm * std::max(per, 1);
+        per = 0;
+        if (f.thr_c == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_comm_kernel<MODE_RK1, 256, true, 8>, 256, G.sm_cm);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_comm_kernel<MODE_RK1, 512, true, 8>, 512, G.sm_cm);
+        G.grid_cm = nsm * std::max(per, 1);
+        per = 0;
+        if (f.thr_c == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_comm_kernel<MODE_RK1, 256, false>, 256, G.sm_cc);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sweep_comm_kernel<MODE_RK1, 512, false>, 512, G.sm_cc);
+        G.grid_cc = nsm * std::max(per, 1);
+    }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(h0, EDUS_ERR_CUDA, std::string("fused sweep set-up: ") + cudaGetErrorString(e));
     return EDUS_OK;
 }
 
+// One group's launches for stage `mode` of one step: planes, then the
+// commutators of each kind.
 template <int MODE>
-static void fused_comm_launch(const FusedSweep& f, const StageArgs* args, int* cnt, cudaStream_t st) {
-    const int4* it = f.items + f.nl + f.ns;
-    if (f.thr_c == 256)
-        sweep_comm_kernel<MODE, 256><<<f.grid_c, 256, f.sm_c, st>>>(args, f.mma, it, f.nc, cnt);
-    else
-        sweep_comm_kernel<MODE, 512><<<f.grid_c, 512, f.sm_c, st>>>(args, f.mma, it, f.nc, cnt);
+static int fused_group_stage(const FusedSweep& f, const FusedGroup& G, const StageArgs* a, int* cnt, cudaStream_t st) {
+    int launched = 0;
+    const int4* ip = f.items + G.off;
+    const int4* im = ip + G.np;
+    const int4* ic = im + G.ncm;
+    if (G.np) {
+        if (G.thr_p == 512) {
+            if (f.wide) sweep_plane_kernel<kRadixAll, 512><<<G.grid_p, 512, G.sm_p, st>>>(f.pdesc, a, ip, G.np, cnt);
+            else sweep_plane_kernel<kRadixCommon, 512><<<G.grid_p, 512, G.sm_p, st>>>(f.pdesc, a, ip, G.np, cnt);
+        } else {
+            if (f.wide) sweep_plane_kernel<kRadixAll, 256><<<G.grid_p, 256, G.sm_p, st>>>(f.pdesc, a, ip, G.np, cnt);
+            else sweep_plane_kernel<kRadixCommon, 256><<<G.grid_p, 256, G.sm_p, st>>>(f.pdesc, a, ip, G.np, cnt);
+        }
+        ++launched;
+    }
+    if (G.ncm) {
+        if (f.thr_c == 256) {
+            if (f.tiles5) sweep_comm_kernel<MODE, 256, true, 5><<<G.grid_cm, 256, G.sm_cm, st>>>(a, im, G.ncm, cnt + 1);
+            else sweep_comm_kernel<MODE, 256, true, 8><<<G.grid_cm, 256, G.sm_cm, st>>>(a, im, G.ncm, cnt + 1);
+        } else {
+            if (f.tiles5) sweep_comm_kernel<MODE, 512, true, 5><<<G.grid_cm, 512, G.sm_cm, st>>>(a, im, G.ncm, cnt + 1);
+            else sweep_comm_kernel<MODE, 512, true, 8><<<G.grid_cm, 512, G.sm_cm, st>>>(a, im, G.ncm, cnt + 1);
+        }
+        ++launched;
+    }
+    if (G.ncc) {
+        if (f.thr_c == 256) sweep_comm_kernel<MODE, 256, false><<<G.grid_cc, 256, G.sm_cc, st>>>(a, ic, G.ncc, cnt + 2);
+        else sweep_comm_kernel<MODE, 512, false><<<G.grid_cc, 512, G.sm_cc, st>>>(a, ic, G.ncc, cnt + 2);
+        ++launched;
+    }
+    return launched;
 }
 
-// `cnt` RK4 steps of every handle of the sweep, all on stream st.
+// Kernel launches of one fused step (all groups, four stages).
+static int fused_launches_per_step(const FusedSweep& f) {
+    int n = 0;
+    for (const FusedGroup& G : f.g) n += (G.np ? 1 : 0) + (G.ncm ? 1 : 0) + (G.ncc ? 1 : 0);
+    return 4 * n;
+}
+
+// `cnt` RK4 steps of every handle of the sweep: group 0 on st, group 1 on
+// the sweep's second stream, forked from and joined into st.
 static int fused_launch_steps(edus_handle* const* hs, const FusedSweep& f, int cnt, cudaStream_t st) {
     edus_handle* h0 = hs[0];
-    if (cudaMemsetAsync(f.count, 0, (size_t)f.C * 4 * 3 * sizeof(int), st) != cudaSuccess)
-        return fail(h0, EDUS_ERR_CUDA, "fused sweep: counter reset failed");
+    if (cudaMemsetAsync(f.count, 0, (size_t)f.C * 4 * 2 * 3 * sizeof(int), st) != cudaSuccess ||
+        cudaEventRecord(f.fork, st) != cudaSuccess || cudaStreamWaitEvent(f.s1, f.fork, 0) != cudaSuccess)
+        return fail(h0, EDUS_ERR_CUDA, "fused sweep: counter reset / fork failed");
     for (int k = 0; k < cnt; ++k) {
         for (int s = 0; s < 4; ++s) {
             const StageArgs* a = f.args + ((size_t)k * 4 + s) * f.n;
-            int* c = f.count + ((size_t)k * 4 + s) * 3;
-            if (f.nl) {
-                if (f.wide) sweep_plane_kernel<kRadixAll, 512><<<f.grid_l, 512, f.sm_l, st>>>(f.pdesc, a, f.items, f.nl, c);
-                else sweep_plane_kernel<kRadixCommon, 512><<<f.grid_l, 512, f.sm_l, st>>>(f.pdesc, a, f.items, f.nl, c);
+            for (int gi = 0; gi < 2; ++gi) {
+                int* c = f.count + (((size_t)k * 4 + s) * 2 + gi) * 3;
+                const cudaStream_t sg = gi == 0 ? st : f.s1;
+                switch (s) {
+                    case 0: fused_group_stage<MODE_RK1>(f, f.g[gi], a, c, sg); break;
+                    case 1: fused_group_stage<MODE_RK2>(f, f.g[gi], a, c, sg); break;
+                    case 2: fused_group_stage<MODE_RK3>(f, f.g[gi], a, c, sg); break;
+                    default: fused_group_stage<MODE_RK4>(f, f.g[gi], a, c, sg); break;
+                }
             }
-            if (f.ns) {
-                const int4* it = f.items + f.nl;
-                if (f.wide) sweep_plane_kernel<kRadixAll, 256><<<f.grid_s, 256, f.sm_s, st>>>(f.pdesc, a, it, f.ns, c + 1);
-                else sweep_plane_kernel<kRadixCommon, 256><<<f.grid_s, 256, f.sm_s, st>>>(f.pdesc, a, it, f.ns, c + 1);
-            }
-            switch (s) {
-                case 0: fused_comm_launch<MODE_RK1>(f, a, c + 2, st); break;
-                case 1: fused_comm_launch<MODE_RK2>(f, a, c + 2, st); break;
-                case 2: fused_comm_launch<MODE_RK3>(f, a, c + 2, st); break;
-                default: fused_comm_launch<MODE_RK4>(f, a, c + 2, st); break;
-            }
-            h0->launches += (f.nl ? 1 : 0) + (f.ns ? 1 : 0) + 1;
         }
         for (int i = 0; i < f.n; ++i) hs[i]->t += hs[i]->d.dt;
+        h0->launches += fused_launches_per_step(f);
     }
+    if (cudaEventRecord(f.join, f.s1) != cudaSuccess || cudaStreamWaitEvent(st, f.join, 0) != cudaSuccess)
+        return fail(h0, EDUS_ERR_CUDA, "fused sweep: join failed");
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(h0, EDUS_ERR_CUDA, std::string("fused sweep launch: ") + cudaGetErrorString(e));
     return EDUS_OK;
@@ -2325,7 +2397,7 @@ int edus_sweep_step(edus_handle* const* hs, int n, int steps, int use_graph) {
                 for (int k = 0; k < C; ++k) hs[i]->t += hs[i]->d.dt;  // as the launches would
                 if (!fused) hs[i]->launches += 8LL * C;
             }
-            if (fused) h0->launches += (unsigned long long)C * 4 * ((fs.nl ? 1 : 0) + (fs.ns ? 1 : 0) + 1);
+            if (fused) h0->launches += (unsigned long long)C * fused_launches_per_step(fs);
         } else {
             rc = launch_all(cnt);
         }

@@ -768,7 +768,7 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 // One (k tile, solve) of the FP64 tensor-core commutator: the body of
 // commutator_mma_kernel, also run by the sweep's persistent commutator kernel.
 // Warps past the first 8 take no product tiles (kk >= TK below).
-template <int MODE, bool COUL, bool FH = false>
+template <int MODE, bool COUL, bool FH = false, int MAXT = 8>
 __device__ __forceinline__ void commutator_mma_tile(const StageArgs& a, int b, int tile, double* smd) {
     const int nb = a.nb, Nk = a.Nk;
     const MmaGeom g = mma_geometry(nb);
@@ -805,7 +805,7 @@ __device__ __forceinline__ void commutator_mma_tile(const StageArgs& a, int b, i
     const int ntile = g.tiles * g.tiles;
     const int per = (ntile + g.warps_per_k - 1) / g.warps_per_k;
     const int t0 = part * per, t1 = min(ntile, t0 + per);
-    constexpr int MAXT = 8;  // tiles per warp (nb <= 64)
+    // MAXT: 8x8 output tiles per warp, at most 8 (nb <= 64); 5 covers nb <= 24
     double cr[MAXT][2], ci[MAXT][2];
 #pragma unroll
     for (int t = 0; t < MAXT; ++t) cr[t][0] = cr[t][1] = ci[t][0] = ci[t][1] = 0.0;

@@ -2,7 +2,8 @@
 // band counts and k grids, independent-particle RHS, FP64, RK4) with one
 // launch per RK stage for the plane transforms of every solve (per shared
 // memory class: planes that leave room for two CTAs on an SM, and larger
-// ones) and one launch for the commutators and stage updates of every solve.
+// ones) and one launch for the commutators and stage updates of every solve
+// (per commutator kind: FP64 tensor cores or CUDA cores).
 //
 // Work items are (shape handle, solve, plane) and (shape handle, solve, k
 // tile), ordered by decreasing cost on the host; a CTA takes the next item of
@@ -42,7 +43,7 @@ __device__ __forceinline__ int sweep_fetch(int* counter, int* slot) {
 // G_k = FFT^-1(G_R).  args[shape] are the shape's stage arguments (stage input
 // rho, field table of the stage).
 template <int MASK, int MAXT>
-__global__ void __launch_bounds__(MAXT) sweep_plane_kernel(const SweepPlaneDesc* __restrict__ descs,
+__global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) sweep_plane_kernel(const SweepPlaneDesc* __restrict__ descs,
                                                            const StageArgs* __restrict__ args,
                                                            const int4* __restrict__ items, int nitems, int* counter) {
     extern __shared__ double2 X[];
@@ -82,23 +83,24 @@ __global__ void __launch_bounds__(MAXT) sweep_plane_kernel(const SweepPlaneDesc*
 }
 
 // Commutator items {shape, solve, k tile}: f = G - i[H0 + E.xi, rho] and the
-// RK stage update of the shape's arrays, on the FP64 tensor cores where the
-// shape's handle uses them (mma[shape] != 0), on CUDA cores otherwise.  MAXT
-// is at least every shape's commutator thread count (256 for fewer than 46
-// bands).
-template <int MODE, int MAXT>
-__global__ void __launch_bounds__(MAXT) sweep_comm_kernel(const StageArgs* __restrict__ args,
-                                                         const int* __restrict__ mma,
-                                                         const int4* __restrict__ items, int nitems, int* counter) {
+// RK stage update of the shape's arrays, on the FP64 tensor cores (MMA, the
+// shapes whose handle uses them) or on CUDA cores (the others): one launch
+// per kind, so that each compiles to the registers of the shape's own kernel.
+// MAXT is at least every shape's commutator thread count (256 for fewer than
+// 46 bands); TILES bounds the 8x8 tiles a warp takes (5 covers 24 bands).
+template <int MODE, int MAXT, bool MMA, int TILES = 8>
+__global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) sweep_comm_kernel(const StageArgs* __restrict__ args,
+                                                                             const int4* __restrict__ items,
+                                                                             int nitems, int* counter) {
     extern __shared__ double2 sm[];
     __shared__ int s_item;
     for (;;) {
         const int w = sweep_fetch(counter, &s_item);
         if (w >= nitems) break;
         const int4 it = items[w];
-        const StageArgs& a = args[it.x];
-        if (mma[it.x])
-            commutator_mma_tile<MODE, false>(a, it.y, it.z, (double*)sm);
+        const StageArgs a = args[it.x];
+        if constexpr (MMA)
+            commutator_mma_tile<MODE, false, false, TILES>(a, it.y, it.z, (double*)sm);
         else
             commutator_tile<MODE, false>(a, it.y, it.z, sm);
     }
