@@ -554,7 +554,7 @@ def run_sweep(args, rank, world, local_rank):
                 s.upload_model_solve(b, m.H0k, m.xik)
             s.set_lasers(m.cfg.lasers, b)
             s.set_state(m.rho0k, b)
-        tune[f"{nb}x{N}x{N}"] = s.autotune()
+        tune[f"{nb}x{N}x{N}"] = s.autotune() if not args.no_autotune else (None, None)
         handles.append(s)
         order.append(idx)
     t_setup = time.perf_counter() - t_setup
@@ -632,6 +632,7 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=4000)
     ap.add_argument("--workload", choices=["tmd22_rk4", "sweep"], default="tmd22_rk4")
     ap.add_argument("--solves", type=int, default=256)
+    ap.add_argument("--no-autotune", action="store_true", help="sweep: keep the default launch variants")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
