@@ -347,6 +347,30 @@ void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long l
             h->ntab, h->flag);
 }
 
+// The three plane3 launches (rows, columns, rows) of one right-hand side.
+template <int MASK>
+void launch_plane3(edus_handle* h, const double2* in, long long in_bstride, double2* G, double2* Hee,
+                   long long out_bstride, const StageField* field, int nbatch, int nS, bool c) {
+    const int planes = h->P * nbatch;
+    const int N0 = h->N[0], N1 = h->N[1];
+    const long long bs = (long long)h->S;
+    dim3 gr(planes, N0 / h->p3.Rc), gc(planes, N1 / h->p3.Cc), gi(planes * (c ? 2 : 1), N0 / h->p3.Rc);
+    const size_t smr = (size_t)h->p3.Rc * N1 * sizeof(double2);
+    const size_t smc = (size_t)N0 * h->p3.Cc * sizeof(double2) * (c ? 2 : 1);
+    plane3_rows_kernel<true, 256, MASK><<<gr, 128, smr, h->stream>>>(in, in_bstride, h->s3a, bs, h->P, h->p3.rows,
+                                                                     1, h->roots, in, h->s3a);
+    if (c)
+        plane3_cols_kernel<true, 256, MASK><<<gc, 128, smc, h->stream>>>(
+            h->s3a, bs, h->s3g, h->s3h, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->p3.cols,
+            h->p3.Cc, h->nb, 1.0 / h->Nk, h->hpos, h->hval, nS);
+    else
+        plane3_cols_kernel<false, 256, MASK><<<gc, 128, smc, h->stream>>>(
+            h->s3a, bs, h->s3g, h->s3h, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->p3.cols,
+            h->p3.Cc, h->nb, 1.0 / h->Nk, h->hpos, h->hval, 0);
+    plane3_rows_kernel<false, 256, MASK><<<gi, 128, smr, h->stream>>>(h->s3g, bs, G, out_bstride, h->P, h->p3.rows,
+                                                                      c ? 2 : 1, h->roots, h->s3h, Hee);
+}
+
 // fuse: with HSEX and a sparse model, Hee receives the whole Hamiltonian
 // H0 + E.xi + Hee (plane kernel) and the commutator reads only it.
 int launch_split(edus_handle* h, const double2* in, double2* G, double2* H, const StageField* field, int nbatch) {
@@ -451,24 +475,10 @@ int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double
     }
     if (h->use3 && h->nO == 0) {
         // rows (k -> R, axis 1), columns (axis 0 both ways + pointwise), rows (R -> k)
-        const int planes = h->P * nbatch;
-        const int N0 = h->N[0], N1 = h->N[1];
-        const long long bs = (long long)h->S;
-        dim3 gr(planes, N0 / h->p3.Rc), gc(planes, N1 / h->p3.Cc), gi(planes * (c ? 2 : 1), N0 / h->p3.Rc);
-        const size_t smr = (size_t)h->p3.Rc * N1 * sizeof(double2);
-        const size_t smc = (size_t)N0 * h->p3.Cc * sizeof(double2) * (c ? 2 : 1);
-        plane3_rows_kernel<true, 256><<<gr, 128, smr, h->stream>>>(in, in_bstride, h->s3a, bs, h->P, h->p3.rows, 1,
-                                                                   h->roots, in, h->s3a);
-        if (c)
-            plane3_cols_kernel<true, 256><<<gc, 128, smc, h->stream>>>(
-                h->s3a, bs, h->s3g, h->s3h, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->p3.cols,
-                h->p3.Cc, h->nb, 1.0 / h->Nk, h->hpos, h->hval, nS);
+        if (h->plane_cfg.variant == 2)
+            launch_plane3<kRadixAll>(h, in, in_bstride, G, Hee, out_bstride, field, nbatch, nS, c);
         else
-            plane3_cols_kernel<false, 256><<<gc, 128, smc, h->stream>>>(
-                h->s3a, bs, h->s3g, h->s3h, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->p3.cols,
-                h->p3.Cc, h->nb, 1.0 / h->Nk, h->hpos, h->hval, 0);
-        plane3_rows_kernel<false, 256><<<gi, 128, smr, h->stream>>>(h->s3g, bs, G, out_bstride, h->P, h->p3.rows,
-                                                                    c ? 2 : 1, h->roots, h->s3h, Hee);
+            launch_plane3<kRadixCommon>(h, in, in_bstride, G, Hee, out_bstride, field, nbatch, nS, c);
         h->launches += 3;
         if (kmode) launch_kgrad();
         CU(h, cudaGetLastError());
@@ -1267,10 +1277,14 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
             TRY_ALLOC(h->s3a, SBb);
             TRY_ALLOC(h->s3g, SBb);
             if (d.coulomb) TRY_ALLOC(h->s3h, SBb);
-            if ((rc = set_smem(h, plane3_rows_kernel<true, 256>, Rc * h->N[1] * (int)sizeof(double2)))) return bail(rc);
-            if ((rc = set_smem(h, plane3_rows_kernel<false, 256>, Rc * h->N[1] * (int)sizeof(double2)))) return bail(rc);
-            if ((rc = set_smem(h, plane3_cols_kernel<true, 256>, 2 * h->N[0] * Cc * (int)sizeof(double2)))) return bail(rc);
-            if ((rc = set_smem(h, plane3_cols_kernel<false, 256>, h->N[0] * Cc * (int)sizeof(double2)))) return bail(rc);
+            if ((rc = set_smem(h, plane3_rows_kernel<true, 256, kRadixAll>, Rc * h->N[1] * (int)sizeof(double2)))) return bail(rc);
+            if ((rc = set_smem(h, plane3_rows_kernel<false, 256, kRadixAll>, Rc * h->N[1] * (int)sizeof(double2)))) return bail(rc);
+            if ((rc = set_smem(h, plane3_cols_kernel<true, 256, kRadixAll>, 2 * h->N[0] * Cc * (int)sizeof(double2)))) return bail(rc);
+            if ((rc = set_smem(h, plane3_cols_kernel<false, 256, kRadixAll>, h->N[0] * Cc * (int)sizeof(double2)))) return bail(rc);
+            if ((rc = set_smem(h, plane3_rows_kernel<true, 256, kRadixCommon>, Rc * h->N[1] * (int)sizeof(double2)))) return bail(rc);
+            if ((rc = set_smem(h, plane3_rows_kernel<false, 256, kRadixCommon>, Rc * h->N[1] * (int)sizeof(double2)))) return bail(rc);
+            if ((rc = set_smem(h, plane3_cols_kernel<true, 256, kRadixCommon>, 2 * h->N[0] * Cc * (int)sizeof(double2)))) return bail(rc);
+            if ((rc = set_smem(h, plane3_cols_kernel<false, 256, kRadixCommon>, h->N[0] * Cc * (int)sizeof(double2)))) return bail(rc);
             h->use3 = true;
         }
     }
@@ -1956,6 +1970,7 @@ struct FusedSweep {
     PlanePlan* plans = nullptr;
     SweepPlaneDesc* pdesc = nullptr;
     StageArgs* args = nullptr;  // [C][4][n]: handle i at step k of a chunk, stage s
+    std::vector<StageArgs> host_args;  // the same on the host (the commutators take them as a parameter)
     int4* items = nullptr;      // per group: planes | tensor-core tiles | CUDA-core tiles
     FusedGroup g[2];            // 0: planes above 110 KB, 1: the others
     int thr_c = 256;
@@ -1992,6 +2007,9 @@ static bool fused_eligible(const edus_handle* h) {
 
 static int fused_setup(edus_handle* const* hs, int n, int C, FusedSweep& f) {
     edus_handle* h0 = hs[0];
+    if (n > kSweepMaxShapes)
+        return fail(h0, EDUS_ERR_UNSUPPORTED,
+                    "the fused sweep takes at most " + std::to_string(kSweepMaxShapes) + " handles");
     f.n = n;
     f.C = C;
     std::vector<PlanePlan> plans(n);
@@ -2071,6 +2089,7 @@ static int fused_setup(edus_handle* const* hs, int n, int C, FusedSweep& f) {
     }
     if ((rc = alloc_copy((void**)&f.pdesc, pd.data(), n * sizeof(SweepPlaneDesc)))) return rc;
     if ((rc = alloc_copy((void**)&f.args, args.data(), args.size() * sizeof(StageArgs)))) return rc;
+    f.host_args = args;
     if ((rc = alloc_copy((void**)&f.items, items.data(), std::max<size_t>(items.size(), 1) * sizeof(int4)))) return rc;
     if ((rc = alloc_copy((void**)&f.count, nullptr, (size_t)C * 4 * 2 * 3 * sizeof(int)))) return rc;
     if (cudaStreamCreateWithFlags(&f.s1, cudaStreamNonBlocking) != cudaSuccess ||
@@ -2127,7 +2146,8 @@ static int fused_setup(edus_handle* const* hs, int n, int C, FusedSweep& f) {
 // One group's launches for stage `mode` of one step: planes, then the
 // commutators of each kind.
 template <int MODE>
-static int fused_group_stage(const FusedSweep& f, const FusedGroup& G, const StageArgs* a, int* cnt, cudaStream_t st) {
+static int fused_group_stage(const FusedSweep& f, const FusedGroup& G, const StageArgs* a,
+                             const SweepStageArgs& pa, int* cnt, cudaStream_t st) {
     int launched = 0;
     const int4* ip = f.items + G.off;
     const int4* im = ip + G.np;
@@ -2144,17 +2164,17 @@ static int fused_group_stage(const FusedSweep& f, const FusedGroup& G, const Sta
     }
     if (G.ncm) {
         if (f.thr_c == 256) {
-            if (f.tiles5) sweep_comm_kernel<MODE, 256, true, 5><<<G.grid_cm, 256, G.sm_cm, st>>>(a, im, G.ncm, cnt + 1);
-            else sweep_comm_kernel<MODE, 256, true, 8><<<G.grid_cm, 256, G.sm_cm, st>>>(a, im, G.ncm, cnt + 1);
+            if (f.tiles5) sweep_comm_kernel<MODE, 256, true, 5><<<G.ncm, 256, G.sm_cm, st>>>(pa, im);
+            else sweep_comm_kernel<MODE, 256, true, 8><<<G.ncm, 256, G.sm_cm, st>>>(pa, im);
         } else {
-            if (f.tiles5) sweep_comm_kernel<MODE, 512, true, 5><<<G.grid_cm, 512, G.sm_cm, st>>>(a, im, G.ncm, cnt + 1);
-            else sweep_comm_kernel<MODE, 512, true, 8><<<G.grid_cm, 512, G.sm_cm, st>>>(a, im, G.ncm, cnt + 1);
+            if (f.tiles5) sweep_comm_kernel<MODE, 512, true, 5><<<G.ncm, 512, G.sm_cm, st>>>(pa, im);
+            else sweep_comm_kernel<MODE, 512, true, 8><<<G.ncm, 512, G.sm_cm, st>>>(pa, im);
         }
         ++launched;
     }
     if (G.ncc) {
-        if (f.thr_c == 256) sweep_comm_kernel<MODE, 256, false><<<G.grid_cc, 256, G.sm_cc, st>>>(a, ic, G.ncc, cnt + 2);
-        else sweep_comm_kernel<MODE, 512, false><<<G.grid_cc, 512, G.sm_cc, st>>>(a, ic, G.ncc, cnt + 2);
+        if (f.thr_c == 256) sweep_comm_kernel<MODE, 256, false><<<G.ncc, 256, G.sm_cc, st>>>(pa, ic);
+        else sweep_comm_kernel<MODE, 512, false><<<G.ncc, 512, G.sm_cc, st>>>(pa, ic);
         ++launched;
     }
     return launched;
@@ -2174,17 +2194,20 @@ static int fused_launch_steps(edus_handle* const* hs, const FusedSweep& f, int c
     if (cudaMemsetAsync(f.count, 0, (size_t)f.C * 4 * 2 * 3 * sizeof(int), st) != cudaSuccess ||
         cudaEventRecord(f.fork, st) != cudaSuccess || cudaStreamWaitEvent(f.s1, f.fork, 0) != cudaSuccess)
         return fail(h0, EDUS_ERR_CUDA, "fused sweep: counter reset / fork failed");
+    static SweepStageArgs pa;  // launch parameter, copied at each launch
     for (int k = 0; k < cnt; ++k) {
         for (int s = 0; s < 4; ++s) {
             const StageArgs* a = f.args + ((size_t)k * 4 + s) * f.n;
+            const StageArgs* ha = f.host_args.data() + ((size_t)k * 4 + s) * f.n;
+            for (int i = 0; i < f.n; ++i) pa.a[i] = ha[i];
             for (int gi = 0; gi < 2; ++gi) {
                 int* c = f.count + (((size_t)k * 4 + s) * 2 + gi) * 3;
                 const cudaStream_t sg = gi == 0 ? st : f.s1;
                 switch (s) {
-                    case 0: fused_group_stage<MODE_RK1>(f, f.g[gi], a, c, sg); break;
-                    case 1: fused_group_stage<MODE_RK2>(f, f.g[gi], a, c, sg); break;
-                    case 2: fused_group_stage<MODE_RK3>(f, f.g[gi], a, c, sg); break;
-                    default: fused_group_stage<MODE_RK4>(f, f.g[gi], a, c, sg); break;
+                    case 0: fused_group_stage<MODE_RK1>(f, f.g[gi], a, pa, c, sg); break;
+                    case 1: fused_group_stage<MODE_RK2>(f, f.g[gi], a, pa, c, sg); break;
+                    case 2: fused_group_stage<MODE_RK3>(f, f.g[gi], a, pa, c, sg); break;
+                    default: fused_group_stage<MODE_RK4>(f, f.g[gi], a, pa, c, sg); break;
                 }
             }
         }

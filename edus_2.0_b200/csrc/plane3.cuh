@@ -10,6 +10,7 @@
 // A stage transforms whole lines of one axis of a [outer][n][inner] sub-array
 // (fft_plane.cuh's stage indexing is generic in Nk, n and inner), so the
 // sub-plans below reuse the plane's radices, roots and coordinate tables.
+// MASK: the radices compiled in (the common set unless the plan needs 11 or 13).
 // Reference: Functional_SourceTerm.hpp:15-50, kGradient_definitions.hpp:35-40,
 // Coulomb.cpp:150-171, fftPair.cpp:89-107.
 #pragma once
@@ -50,7 +51,7 @@ inline Plane3Plan plane3_plan(const PlanePlan& full, int Rc, int Cc) {
 // rows: dst[plane][r][*] = FFT along axis 1 (FWD: k -> R) of src rows of the
 // CTA's chunk; with nout = 2 the CTAs alternate between (src, dst) and
 // (src2, dst2) (the G and H planes of the inverse pass)
-template <bool FWD, int MAXT>
+template <bool FWD, int MAXT, int MASK = kRadixAll>
 __global__ void __launch_bounds__(MAXT) plane3_rows_kernel(const double2* __restrict__ src, long long src_bstride,
                                                          double2* __restrict__ dst, long long dst_bstride, int P,
                                                          PlanePlan sub, int nout, const double2* __restrict__ roots,
@@ -66,13 +67,13 @@ __global__ void __launch_bounds__(MAXT) plane3_rows_kernel(const double2* __rest
     double2* d = which ? dst2 : dst;
     for (int i = threadIdx.x; i < sub.Nk; i += blockDim.x) x3[i] = __ldg(&s[so + i]);
     __syncthreads();
-    if (FWD) plane_forward<1, kRadixAll>(x3, 0, sub, roots);
-    else plane_inverse<1, kRadixAll>(x3, 0, sub, roots);
+    if (FWD) plane_forward<1, MASK>(x3, 0, sub, roots);
+    else plane_inverse<1, MASK>(x3, 0, sub, roots);
     for (int i = threadIdx.x; i < sub.Nk; i += blockDim.x) d[dof + i] = x3[i];
 }
 
 // columns: k -> R along axis 0, pointwise terms, R -> k along axis 0 of G (and H)
-template <bool COUL, int MAXT>
+template <bool COUL, int MAXT, int MASK = kRadixAll>
 __global__ void __launch_bounds__(MAXT) plane3_cols_kernel(
     const double2* __restrict__ S1, long long bstride, double2* __restrict__ SG, double2* __restrict__ SH,
     const double2* __restrict__ rho0p, const double* __restrict__ Wp, double2* __restrict__ diag0,
@@ -94,7 +95,7 @@ __global__ void __launch_bounds__(MAXT) plane3_cols_kernel(
         X[i] = __ldg(&S1[off + (long long)r * N1 + c0 + c]);
     }
     __syncthreads();
-    plane_forward<1, kRadixAll>(X, 0, sub, roots);
+    plane_forward<1, MASK>(X, 0, sub, roots);
     const StageField F = field[b];
     const int n = p / nb, m = p - (p / nb) * nb;
     if (COUL && n == m && c0 == 0 && threadIdx.x == 0) diag0[b * nb + n] = cscale(X[0], inv_nk);
@@ -138,8 +139,8 @@ __global__ void __launch_bounds__(MAXT) plane3_cols_kernel(
         }
         __syncthreads();
     }
-    if (COUL) plane_inverse<2, kRadixAll>(X, tot, sub, roots);
-    else plane_inverse<1, kRadixAll>(X, 0, sub, roots);
+    if (COUL) plane_inverse<2, MASK>(X, tot, sub, roots);
+    else plane_inverse<1, MASK>(X, 0, sub, roots);
     for (int i = threadIdx.x; i < tot; i += blockDim.x) {
         const int r = i / Cc, c = i - (i / Cc) * Cc;
         SG[off + (long long)r * N1 + c0 + c] = X[i];

@@ -1,14 +1,18 @@
-// Persistent kernels that advance a whole sweep of uneven solves (different
-// band counts and k grids, independent-particle RHS, FP64, RK4) with one
-// launch per RK stage for the plane transforms of every solve (per shared
-// memory class: planes that leave room for two CTAs on an SM, and larger
-// ones) and one launch for the commutators and stage updates of every solve
-// (per commutator kind: FP64 tensor cores or CUDA cores).
+// Kernels that advance a whole sweep of uneven solves (different band counts
+// and k grids, independent-particle RHS, FP64, RK4) with one launch per RK
+// stage for the plane transforms of every solve (per shared-memory class:
+// planes that leave room for two CTAs on an SM, and larger ones) and one
+// launch for the commutators and stage updates of every solve (per
+// commutator kind: FP64 tensor cores or CUDA cores).
 //
 // Work items are (shape handle, solve, plane) and (shape handle, solve, k
-// tile), ordered by decreasing cost on the host; a CTA takes the next item of
-// its launch from an atomic counter (largest first onto whichever CTA is
-// free), so the solves of small shapes fill the SMs that the large ones leave.
+// tile), ordered by decreasing cost on the host.  The plane kernel is
+// persistent: a CTA takes the next item from an atomic counter (largest first
+// onto whichever CTA is free).  The commutator kernels run one CTA per item in
+// that order (the block scheduler hands items to SMs as they free up), which
+// keeps their code at the registers of the per-shape kernels; their
+// arguments are one launch parameter.  The solves of small shapes fill the SMs
+// that the large ones leave.
 // Each item runs the same device code as the shape's own kernels
 // (plane_forward / plane_inverse with the gradient of kGradient_definitions.hpp:34-40;
 // commutator_tile / commutator_mma_tile with the RK stage epilogue of
@@ -82,28 +86,32 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) sweep_plane_kernel(
     }
 }
 
+// The stage arguments of every shape of a fused sweep, as one launch
+// parameter: item code reads them from the constant bank, as the per-shape
+// kernels read their own StageArgs parameter.
+constexpr int kSweepMaxShapes = 64;
+struct SweepStageArgs {
+    StageArgs a[kSweepMaxShapes];
+};
+
 // Commutator items {shape, solve, k tile}: f = G - i[H0 + E.xi, rho] and the
 // RK stage update of the shape's arrays, on the FP64 tensor cores (MMA, the
 // shapes whose handle uses them) or on CUDA cores (the others): one launch
-// per kind, so that each compiles to the registers of the shape's own kernel.
-// MAXT is at least every shape's commutator thread count (256 for fewer than
-// 46 bands); TILES bounds the 8x8 tiles a warp takes (5 covers 24 bands).
+// per kind over all items, one CTA per item, largest items first (the block
+// scheduler hands them out as SMs free up), so that each compiles to the
+// registers of the shape's own kernel.  MAXT is at least every shape's
+// commutator thread count (256 for fewer than 46 bands); TILES bounds the 8x8
+// tiles a warp takes (5 covers 24 bands).
 template <int MODE, int MAXT, bool MMA, int TILES = 8>
-__global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) sweep_comm_kernel(const StageArgs* __restrict__ args,
-                                                                             const int4* __restrict__ items,
-                                                                             int nitems, int* counter) {
+__global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) sweep_comm_kernel(
+    const __grid_constant__ SweepStageArgs args, const int4* __restrict__ items) {
     extern __shared__ double2 sm[];
-    __shared__ int s_item;
-    for (;;) {
-        const int w = sweep_fetch(counter, &s_item);
-        if (w >= nitems) break;
-        const int4 it = items[w];
-        const StageArgs a = args[it.x];
-        if constexpr (MMA)
-            commutator_mma_tile<MODE, false, false, TILES>(a, it.y, it.z, (double*)sm);
-        else
-            commutator_tile<MODE, false>(a, it.y, it.z, sm);
-    }
+    const int4 it = items[blockIdx.x];
+    const StageArgs& a = args.a[it.x];
+    if constexpr (MMA)
+        commutator_mma_tile<MODE, false, false, TILES>(a, it.y, it.z, (double*)sm);
+    else
+        commutator_tile<MODE, false>(a, it.y, it.z, sm);
 }
 
 }  // namespace edus
