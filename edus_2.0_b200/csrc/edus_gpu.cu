@@ -104,6 +104,7 @@ struct edus_handle {
     int split_grid = 0, split_threads = 256;
     PlaneLaunch plane_cfg{0, 512, false};
     int plane_grid = 0;            // persistent plane kernel: CTAs per launch
+    int wait_polls = 1 << 22;      // the plane kernel's bulk-load wait limit (edus_set_wait_limit)
     double2* plane_scratch = nullptr;  // [plane_grid][Nk]: rho(R) between the two inverse transforms
     unsigned long long launches = 0;
     size_t dev_bytes = 0;
@@ -344,7 +345,7 @@ void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long l
         <<<grid, h->plane_cfg.threads, h->Nk * sizeof(double2) + 16, h->stream>>>(
             in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
             1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0, ptab,
-            h->ntab, h->flag);
+            h->ntab, h->flag, h->wait_polls);
 }
 
 // The three plane3 launches (rows, columns, rows) of one right-hand side.
@@ -2640,6 +2641,12 @@ int edus_population_wannier(edus_handle* h, int b, double* pop) {
 int edus_get_stream(const edus_handle* h, void** stream) {
     if (!h || !stream) return EDUS_ERR_ARG;
     *stream = (void*)h->stream;
+    return EDUS_OK;
+}
+
+int edus_set_wait_limit(edus_handle* h, int polls) {
+    if (!h) return EDUS_ERR_ARG;
+    h->wait_polls = polls > 0 ? polls : (1 << 22);
     return EDUS_OK;
 }
 

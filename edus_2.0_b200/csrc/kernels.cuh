@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     const double2* __restrict__ roots, const double* __restrict__ rpos, PlanePlan pl, int nb, double inv_nk,
     double2* __restrict__ scratch, int nplanes, const int* __restrict__ hpos, const double2* __restrict__ hval,
     int nS, const int* __restrict__ opos, const double2* __restrict__ oval, int nO,
-    const double2* __restrict__ ptab = nullptr, int ntab = 0, int* status = nullptr) {
+    const double2* __restrict__ ptab = nullptr, int ntab = 0, int* status = nullptr, int wait_polls = 1 << 22) {
     extern __shared__ double2 smem[];
     const int Nk = pl.Nk;
     const int P = nb * nb;
@@ -293,13 +293,15 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                     bulk_load((unsigned char*)X + off, (const unsigned char*)src + off, min(32768u, bytes - off),
                               lbar);
             }
-            const bool ok = mbar_wait(lbar, (unsigned)(nload & 1), 1 << 22);
+            const bool ok = mbar_wait(lbar, (unsigned)(nload & 1), wait_polls);
             ++nload;
             if (__syncthreads_or(!ok)) {
-                // give up: report, and let the copy land before the CTA ends
+                // give up: report, and let the copy land (and earlier stores
+                // complete) before the CTA ends; these waits keep the full limit
                 if (threadIdx.x == 0) {
                     if (status) atomicOr(status, 1);
                     mbar_wait(lbar, (unsigned)((nload - 1) & 1), 1 << 22);
+                    bulk_wait_all();
                 }
                 return;
             }

@@ -37,7 +37,7 @@ EXPORTS = [
     "edus_mlp_create", "edus_mlp_destroy", "edus_mlp_last_error", "edus_mlp_param_count", "edus_mlp_set_params",
     "edus_mlp_get_params", "edus_mlp_forward", "edus_mlp_gradients", "edus_mlp_train_step",    "edus_upload_model_solve", "edus_sweep_step", "edus_autotune",
     "edus_upload_observables", "edus_observables", "edus_efield", "edus_set_kgradient",
-    "edus_set_peierls", "edus_vector_potential",
+    "edus_set_peierls", "edus_vector_potential", "edus_set_wait_limit",
 ]
 
 
@@ -117,6 +117,7 @@ def load_library(path: str | None = None):
     L.edus_observables.argtypes = [h, ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.edus_efield.argtypes = [h, ctypes.c_int, ctypes.c_double, dp]
     L.edus_set_peierls.argtypes = [h, ctypes.c_int]
+    L.edus_set_wait_limit.argtypes = [h, ctypes.c_int]
     L.edus_vector_potential.argtypes = [h, ctypes.c_int, ctypes.c_double, dp]
     L.edus_sweep_step.argtypes = [P(h), ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.edus_autotune.argtypes = [h, P(ctypes.c_int), P(ctypes.c_int)]
@@ -333,6 +334,10 @@ class Solver:
         H = _c128(H0k, self.shape)
         X = _c128(xik, (3,) + self.shape)
         self._check(self._L.edus_upload_model_solve(self._h, int(b), _dp(H), _dp(X)))
+
+    def set_wait_limit(self, polls: int):
+        """Poll limit of the plane kernel's bulk-load wait (<= 0: the default)."""
+        self._check(self._L.edus_set_wait_limit(self._h, int(polls)))
 
     def autotune(self):
         """Time the launch variants on this handle's data and keep the fastest;

@@ -288,6 +288,15 @@ int edus_population_wannier(edus_handle* h, int b, double* pop_wannier);
 /* The CUDA stream (cudaStream_t) every kernel of this handle runs on. */
 int edus_get_stream(const edus_handle* h, void** stream);
 
+/* Poll limit of the plane kernel's wait for its bulk-copied plane (planes of
+ * 4096 points and more), in mbarrier polls; polls <= 0 restores the default
+ * (2^22, far above any copy).  A wait that runs out sets the handle's status
+ * word (the CTA still lets its copies land before it ends), and the next
+ * synchronising call returns EDUS_ERR_TIMEOUT and clears the word.  For
+ * exercising the failure path: a limit of 1 makes the waits run out.  No
+ * reference counterpart. */
+int edus_set_wait_limit(edus_handle* h, int polls);
+
 /* Per-kernel timing with CUDA events on the handle's stream (off by default).
  * kind 0 = plane kernel (k<->R transforms + gradient + HSEX), 1 = commutator
  * + stage kernel.  Totals accumulate from the call that enabled profiling;
