@@ -2646,7 +2646,7 @@ int edus_get_stream(const edus_handle* h, void** stream) {
 
 int edus_set_wait_limit(edus_handle* h, int polls) {
     if (!h) return EDUS_ERR_ARG;
-    h->wait_polls = polls > 0 ? polls : (1 << 22);
+    h->wait_polls = polls >= 0 ? polls : (1 << 22);
     return EDUS_OK;
 }
 

@@ -336,7 +336,7 @@ class Solver:
         self._check(self._L.edus_upload_model_solve(self._h, int(b), _dp(H), _dp(X)))
 
     def set_wait_limit(self, polls: int):
-        """Poll limit of the plane kernel's bulk-load wait (<= 0: the default)."""
+        """Poll limit of the plane kernel's bulk-load wait (< 0: the default; 0 gives up at once)."""
         self._check(self._L.edus_set_wait_limit(self._h, int(polls)))
 
     def autotune(self):

@@ -289,12 +289,12 @@ int edus_population_wannier(edus_handle* h, int b, double* pop_wannier);
 int edus_get_stream(const edus_handle* h, void** stream);
 
 /* Poll limit of the plane kernel's wait for its bulk-copied plane (planes of
- * 4096 points and more), in mbarrier polls; polls <= 0 restores the default
- * (2^22, far above any copy).  A wait that runs out sets the handle's status
- * word (the CTA still lets its copies land before it ends), and the next
- * synchronising call returns EDUS_ERR_TIMEOUT and clears the word.  For
- * exercising the failure path: a limit of 1 makes the waits run out.  No
- * reference counterpart. */
+ * 4096 points and more), in mbarrier try-waits (each of which may itself
+ * block for a while); polls < 0 restores the default (2^22, far above any
+ * copy).  A wait that runs out sets the handle's status word (the CTA still
+ * lets its copies land before it ends), and the next synchronising call
+ * returns EDUS_ERR_TIMEOUT and clears the word.  For exercising the failure
+ * path: a limit of 0 gives up without waiting.  No reference counterpart. */
 int edus_set_wait_limit(edus_handle* h, int polls);
 
 /* Per-kernel timing with CUDA events on the handle's stream (off by default).

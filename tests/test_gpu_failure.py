@@ -1,7 +1,7 @@
 """Failure detection on the GPU without a GPU fault.
 
 The plane kernel's wait for its bulk-copied plane is bounded.  With the limit
-lowered to one poll (edus_set_wait_limit) the waits run out: the kernel sets the
+set to zero polls (edus_set_wait_limit) the waits run out: the kernel sets the
 handle's status word, lets its copies land and returns; the next synchronising
 call reports EDUS_ERR_TIMEOUT and clears the word; the handle, given its state
 again, propagates correctly afterwards.  Nothing faults, traps or hangs.
@@ -21,14 +21,14 @@ def test_plane_wait_timeout_is_reported_and_handle_recovers(pkg, po, tmp_path):
     inp = model_input(pkg, tmp_path, "timeout", (72, 64, 1), nb=13, dt=0.01, envelope="gauss")
     cfg, o, s = make_pair(pkg, po, inp)
     rho0 = o.get("rho")
-    s.set_wait_limit(1)
+    s.set_wait_limit(0)
     with pytest.raises(E.EdusError) as ei:
         s.step(2)
         s.synchronize()
     assert ei.value.code == 3  # EDUS_ERR_TIMEOUT
     assert "bounded wait" in str(ei.value)
     s.synchronize()  # the status word was cleared once reported
-    s.set_wait_limit(0)
+    s.set_wait_limit(-1)
     s.set_state(rho0)
     s.time = 0.0
     s.step(5)
