@@ -5,7 +5,7 @@
 // output.  Weights are kept in FP32 (the optimiser's master copy) and in BF16
 // (what the tensor cores multiply); activations are FP32 and are rounded to
 // BF16 as the operand of the next product; every product accumulates in FP32
-// (mma.sync.m16n8k16.f32.bf16.bf16.f32).  Loss: mean squared error over the
+// in tensor memory (tcgen05.mma kind::f16, 128 x 128 tiles).  Loss: mean squared error over the
 // batch and the outputs.  Optimiser: Adam.
 //
 // Layouts: a batch of B samples is row-major [B][features]; a weight matrix is
@@ -25,91 +25,153 @@ namespace {
 constexpr int kLayers = 4;  // three hidden layers and the output layer
 
 // ---------------------------------------------------------------------------
-// C[M][N] (+)= op(A)[M][K] op(B)[K][N], FP32 accumulate.  A(i, k) =
-// A[i * a_rs + k * a_cs], B(k, j) = B[k * b_rs + j * b_cs] (BF16), so a
-// transposed operand is only a change of strides.  Tiles of 64 x 64 with K
-// steps of 16, four warps of 32 x 32 (2 x 4 m16n8 fragments).  Out-of-range
-// rows, columns and K are read as zero and not written.
-constexpr int TM = 64, TN = 64, TKK = 16;
+// C[M][N] (+)= op(A)[M][K] op(B)[K][N] on the 5th-generation tensor cores
+// (tcgen05.mma kind::f16, BF16 operands, FP32 accumulator in tensor memory).
+// A(i, k) = A[i * a_rs + k * a_cs], B(k, j) = B[k * b_rs + j * b_cs] (BF16), so
+// a transposed operand is only a change of strides.
+//
+// A CTA of 4 warps owns a 128 x 128 tile of C, accumulated in 128 TMEM columns
+// (lane = row, column = output column).  K runs in chunks of 64: the 128 threads
+// gather A's 128 x 64 and B's 64 x 128 chunk from global memory (strided,
+// out-of-range rows, columns and K read as zero) into shared memory in the
+// K-major, non-swizzled layout of the tensor-core operand descriptors: 8 rows x
+// 16 bytes per core matrix, core matrices of one 8-row group contiguous along K
+// (leading byte offset 128 B), 8-row groups 1024 B apart (stride byte offset).
+// One thread issues the chunk's four 128 x 128 x 16 MMAs and commits them to an
+// mbarrier, which every thread waits on (bounded) before the next chunk
+// overwrites the operands.  Epilogue: each warp reads its 32 TMEM lanes
+// (tcgen05.ld 32x32b, 8 columns at a time), adds the bias, writes C.
+constexpr int UM = 128, UN = 128, UK = 64;
+constexpr int TM = UM, TN = UN;
+// instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N, M
+constexpr unsigned kUmmaIdesc =
+    (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(UN >> 3) << 17) | ((unsigned)(UM >> 4) << 24);
 
-__device__ __forceinline__ unsigned pack_bf16(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-    const unsigned short l = *reinterpret_cast<unsigned short*>(&lo);
-    const unsigned short h = *reinterpret_cast<unsigned short*>(&hi);
-    return (unsigned)l | ((unsigned)h << 16);
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// shared-memory operand descriptor (K-major, no swizzle, descriptor version 1)
+__device__ __forceinline__ unsigned long long umma_desc(const void* p) {
+    return (unsigned long long)((smem_addr(p) >> 4) & 0x3FFFu) | ((unsigned long long)(128u >> 4) << 16) |
+           ((unsigned long long)(1024u >> 4) << 32) | (1ull << 46);
+}
+
+// element offset of (row r, k) of a 64-wide K chunk in the core-matrix layout
+__device__ __forceinline__ int umma_off(int r, int k) { return (r >> 3) * 512 + (k >> 3) * 64 + (r & 7) * 8 + (k & 7); }
+
+__device__ __forceinline__ bool mbar_wait_parity(unsigned long long* bar, unsigned parity, int limit) {
+    for (int i = 0; i < limit; ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
 }
 
 __global__ void __launch_bounds__(128) gemm_bf16_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A,
                                                        long long a_rs, long long a_cs,
                                                        const __nv_bfloat16* __restrict__ B, long long b_rs,
                                                        long long b_cs, float* __restrict__ C, int ldc,
-                                                       const float* __restrict__ bias, int accumulate) {
-    __shared__ __nv_bfloat16 As[TM][TKK + 8];  // [row][k], padded
-    __shared__ __nv_bfloat16 Bs[TN][TKK + 8];  // [col][k], padded
-    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+                                                       const float* __restrict__ bias, int accumulate,
+                                                       int* __restrict__ status) {
+    __shared__ __align__(1024) __nv_bfloat16 As[UM * UK];  // 16 KB
+    __shared__ __align__(1024) __nv_bfloat16 Bs[UN * UK];  // 16 KB
+    __shared__ __align__(8) unsigned long long mbar;
+    __shared__ unsigned tmem_slot;
+    const int m0 = blockIdx.y * UM, n0 = blockIdx.x * UN;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int g = lane >> 2, tg = lane & 3;
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
-    const __nv_bfloat16 zero = __float2bfloat16(0.f);
-    for (int k0 = 0; k0 < K; k0 += TKK) {
-        for (int e = threadIdx.x; e < TM * TKK; e += blockDim.x) {
-            const int r = e / TKK, k = e - (e / TKK) * TKK;
-            const int gi = m0 + r, gk = k0 + k;
-            As[r][k] = (gi < M && gk < K) ? A[gi * a_rs + gk * a_cs] : zero;
-        }
-        for (int e = threadIdx.x; e < TN * TKK; e += blockDim.x) {
-            const int c = e / TKK, k = e - (e / TKK) * TKK;
-            const int gj = n0 + c, gk = k0 + k;
-            Bs[c][k] = (gj < N && gk < K) ? B[gk * b_rs + gj * b_cs] : zero;
-        }
-        __syncthreads();
-        unsigned af[2][4], bfr[4][2];
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const int r = wm + i * 16 + g;
-            af[i][0] = pack_bf16(As[r][tg * 2], As[r][tg * 2 + 1]);
-            af[i][1] = pack_bf16(As[r + 8][tg * 2], As[r + 8][tg * 2 + 1]);
-            af[i][2] = pack_bf16(As[r][tg * 2 + 8], As[r][tg * 2 + 9]);
-            af[i][3] = pack_bf16(As[r + 8][tg * 2 + 8], As[r + 8][tg * 2 + 9]);
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int c = wn + j * 8 + g;
-            bfr[j][0] = pack_bf16(Bs[c][tg * 2], Bs[c][tg * 2 + 1]);
-            bfr[j][1] = pack_bf16(Bs[c][tg * 2 + 8], Bs[c][tg * 2 + 9]);
-        }
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                asm volatile(
-                    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-                    "{%0,%1,%2,%3};\n"
-                    : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-                    : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bfr[j][0]), "r"(bfr[j][1]));
-        __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_addr(&tmem_slot)),
+                     "r"(UN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(&mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const unsigned tmem = tmem_slot;
+    const __nv_bfloat16 zero = __float2bfloat16(0.f);
+    unsigned phase = 0;
+    bool ok = true;
+    for (int k0 = 0; k0 < K; k0 += UK) {
+        for (int e = threadIdx.x; e < UM * UK; e += blockDim.x) {
+            const int r = e / UK, k = e - (e / UK) * UK;
+            const int gi = m0 + r, gk = k0 + k;
+            As[umma_off(r, k)] = (gi < M && gk < K) ? A[gi * a_rs + gk * a_cs] : zero;
+        }
+        for (int e = threadIdx.x; e < UN * UK; e += blockDim.x) {
+            const int c = e / UK, k = e - (e / UK) * UK;
+            const int gj = n0 + c, gk = k0 + k;
+            Bs[umma_off(c, k)] = (gj < N && gk < K) ? B[gk * b_rs + gj * b_cs] : zero;
+        }
+        // the operands were written by the generic proxy; the tensor core reads them by the async proxy
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+            for (int st = 0; st < UK / 16; ++st) {
+                const unsigned long long da = umma_desc(As + st * 128);  // two core matrices = 16 of K
+                const unsigned long long db = umma_desc(Bs + st * 128);
+                const unsigned accum = (k0 > 0 || st > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(kUmmaIdesc), "r"(accum)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_addr(&mbar))
+                         : "memory");
+        }
+        // the MMAs have read the operands (and written TMEM) once the phase completes
+        if (!mbar_wait_parity(&mbar, phase, 1 << 24)) {
+            // give up: report, wait (bounded again) for the MMAs in flight, skip the rest
+            ok = false;
+            mbar_wait_parity(&mbar, phase, 1 << 24);
+        }
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        if (__syncthreads_or(!ok)) {
+            ok = false;
+            break;
+        }
+    }
+    if (!ok && threadIdx.x == 0 && status) atomicOr(status, 1);
+    // epilogue: TMEM lanes 32 warp .. 32 warp + 31 are this warp's rows
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < (ok ? UN : 0); c0 += 8) {
+        unsigned v[8];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+            : "r"(tmem + ((unsigned)(warp * 32) << 16) + (unsigned)c0));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (row < M) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const int row = m0 + wm + i * 16 + g + (r >= 2 ? 8 : 0);
-                const int col = n0 + wn + j * 8 + tg * 2 + (r & 1);
-                if (row < M && col < N) {
-                    float v = acc[i][j][r];
-                    if (bias) v += bias[col];
+            for (int j = 0; j < 8; ++j) {
+                const int col = n0 + c0 + j;
+                if (col < N) {
+                    float x = __uint_as_float(v[j]);
+                    if (bias) x += bias[col];
                     float* dst = C + (long long)row * ldc + col;
-                    *dst = accumulate ? *dst + v : v;
+                    *dst = accumulate ? *dst + x : x;
                 }
             }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(UN) : "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -211,6 +273,7 @@ struct edus_mlp {
     float* dz = nullptr;
     __nv_bfloat16* dzb = nullptr;
     float* loss = nullptr;
+    int* status = nullptr;  // set when a GEMM's bounded wait for its tensor-core MMAs ran out
     cudaStream_t stream = nullptr;
 };
 
@@ -229,10 +292,22 @@ int mfail(edus_mlp* m, int code, const std::string& msg) {
         if (e_ != cudaSuccess) return mfail(m, EDUS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
+// After a synchronisation: report (and clear) a GEMM wait that ran out.
+int mlp_status(edus_mlp* m) {
+    int v = 0;
+    MCU(m, cudaMemcpy(&v, m->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (v) {
+        MCU(m, cudaMemset(m->status, 0, sizeof(int)));
+        return mfail(m, EDUS_ERR_TIMEOUT, "a bounded wait for the tensor-core MMAs of a GEMM ran out");
+    }
+    return EDUS_OK;
+}
+
 void gemm(edus_mlp* mm, int M, int N, int K, const __nv_bfloat16* A, long long a_rs, long long a_cs,
           const __nv_bfloat16* B, long long b_rs, long long b_cs, float* C, int ldc, const float* bias) {
     dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM);
-    gemm_bf16_kernel<<<grid, 128, 0, mm->stream>>>(M, N, K, A, a_rs, a_cs, B, b_rs, b_cs, C, ldc, bias, 0);
+    gemm_bf16_kernel<<<grid, 128, 0, mm->stream>>>(M, N, K, A, a_rs, a_cs, B, b_rs, b_cs, C, ldc, bias, 0,
+                                                   mm->status);
 }
 
 int ensure_cap(edus_mlp* m, int B) {
@@ -325,7 +400,9 @@ int edus_mlp_create(int n_in, int n_hidden, int n_out, unsigned long long seed, 
         cudaMalloc((void**)&m->m, off * sizeof(float)) != cudaSuccess ||
         cudaMalloc((void**)&m->v, off * sizeof(float)) != cudaSuccess ||
         cudaMalloc((void**)&m->wbf, off * sizeof(__nv_bfloat16)) != cudaSuccess ||
-        cudaMalloc((void**)&m->loss, sizeof(float)) != cudaSuccess) {
+        cudaMalloc((void**)&m->loss, sizeof(float)) != cudaSuccess ||
+        cudaMalloc((void**)&m->status, sizeof(int)) != cudaSuccess ||
+        cudaMemset(m->status, 0, sizeof(int)) != cudaSuccess) {
         edus_mlp_destroy(m);
         return mfail(nullptr, EDUS_ERR_NOMEM, "MLP device allocation failed");
     }
@@ -359,6 +436,7 @@ int edus_mlp_destroy(edus_mlp* m) {
     cudaFree(m->v);
     cudaFree(m->wbf);
     cudaFree(m->loss);
+    cudaFree(m->status);
     for (int l = 0; l < kLayers; ++l) {
         cudaFree(m->z[l]);
         cudaFree(m->a[l]);
@@ -406,7 +484,7 @@ int edus_mlp_forward(edus_mlp* m, int batch, const float* x, float* y) {
                            cudaMemcpyDeviceToDevice, m->stream));
     MCU(m, cudaGetLastError());
     MCU(m, cudaStreamSynchronize(m->stream));
-    return EDUS_OK;
+    return mlp_status(m);
 }
 
 int edus_mlp_gradients(edus_mlp* m, int batch, const float* x, const float* target, float* grads_host,
@@ -422,7 +500,7 @@ int edus_mlp_gradients(edus_mlp* m, int batch, const float* x, const float* targ
         MCU(m, cudaMemcpyAsync(grads_host, m->grads, m->nparams * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
     if (loss_host) MCU(m, cudaMemcpyAsync(loss_host, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
     MCU(m, cudaStreamSynchronize(m->stream));
-    return EDUS_OK;
+    return mlp_status(m);
 }
 
 int edus_mlp_train_step(edus_mlp* m, int batch, const float* x, const float* target, float lr, float* loss_host) {
@@ -441,6 +519,7 @@ int edus_mlp_train_step(edus_mlp* m, int batch, const float* x, const float* tar
     if (loss_host) {
         MCU(m, cudaMemcpyAsync(loss_host, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
         MCU(m, cudaStreamSynchronize(m->stream));
+        return mlp_status(m);
     }
     return EDUS_OK;
 }

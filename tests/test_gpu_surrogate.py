@@ -69,11 +69,14 @@ def test_fock_override_exact_on_all_R(pkg, po, tmp_path):
     assert rel(s.rhs(t, rho), o.rhs(t, rho)) < 1e-10
 
 
-def test_mlp_forward_and_gradients_match_cpu_checker(pkg):
+# (n_in, n_out, batch): single and multiple 128-wide tiles of the tensor-core
+# GEMM in M and N, K chunks of 64 partly filled
+@pytest.mark.parametrize("n_in,n_out,batch", [(37, 21, 300), (300, 260, 129)])
+def test_mlp_forward_and_gradients_match_cpu_checker(pkg, n_in, n_out, batch):
     sur = pkg.surrogate
     rng = np.random.default_rng(3)
-    net = sur.MLP(37, 21, hidden=128, seed=5)
-    dims = [37, 128, 128, 128, 21]
+    net = sur.MLP(n_in, n_out, hidden=128, seed=5)
+    dims = [n_in, 128, 128, 128, n_out]
     p = net.params()
     assert p.size == net.nparams == sum(dims[i] * dims[i + 1] + dims[i + 1] for i in range(4))
     # non-zero biases so that every term is exercised
@@ -83,8 +86,8 @@ def test_mlp_forward_and_gradients_match_cpu_checker(pkg):
         p[off:off + dims[i + 1]] = rng.normal(scale=0.1, size=dims[i + 1])
         off += dims[i + 1]
     net.set_params(p)
-    x = rng.normal(size=(300, 37)).astype(np.float32)
-    t = rng.normal(size=(300, 21)).astype(np.float32)
+    x = rng.normal(size=(batch, n_in)).astype(np.float32)
+    t = rng.normal(size=(batch, n_out)).astype(np.float32)
     y_gpu = net.forward(x).cpu().numpy()
     y_ref = mlp_ref.forward(p, dims, x)[0]
     assert np.abs(y_gpu - y_ref).max() < 1e-2 * np.abs(y_ref).max()
