@@ -19,7 +19,7 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libedus_gpu.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["edus_gpu.cu", "edus_noalloc.cu", "surrogate.cu"]
-HEADERS = ["comm_ws.cuh", "fft_plane.cuh", "kernels.cuh", "packed_kernels.cuh", "plane3.cuh", "plane_plan.hpp", "split_kernels.cuh", "tma.cuh"]
+HEADERS = ["comm_ws.cuh", "fft_plane.cuh", "kernels.cuh", "packed_kernels.cuh", "plane3.cuh", "plane_plan.hpp", "split_kernels.cuh", "sweep_kernels.cuh", "tma.cuh"]
 
 
 def nvcc() -> str:

@@ -104,6 +104,8 @@ struct edus_handle {
     int split_grid = 0, split_threads = 256;
     PlaneLaunch plane_cfg{0, 512, false};
     int plane_grid = 0;            // persistent plane kernel: CTAs per launch
+    int nroot_s = 0, nrpos_s = 0;  // persistent plane kernel: root / coordinate entries it stages in shared memory
+    int tab_smem = 0;              // their bytes (0: read from global memory)
     int wait_polls = 1 << 22;      // the plane kernel's bulk-load wait limit (edus_set_wait_limit)
     double2* plane_scratch = nullptr;  // [plane_grid][Nk]: rho(R) between the two inverse transforms
     unsigned long long launches = 0;
@@ -342,10 +344,10 @@ void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long l
                           const double2* ptab = nullptr) {
     const int grid = std::min(nplanes, h->plane_grid);
     plane_rhs_persist_kernel<COUL, MASK, MAXT, BT>
-        <<<grid, h->plane_cfg.threads, h->Nk * sizeof(double2) + 16, h->stream>>>(
+        <<<grid, h->plane_cfg.threads, h->Nk * sizeof(double2) + 16 + h->tab_smem, h->stream>>>(
             in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
             1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0, ptab,
-            h->ntab, h->flag, h->wait_polls);
+            h->ntab, h->flag, h->wait_polls, h->nroot_s, h->nrpos_s);
 }
 
 // The three plane3 launches (rows, columns, rows) of one right-hand side.
@@ -1166,7 +1168,17 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
         h->plane_grid = 2 * std::max(nsm, 1);
     }
     {
-        const int ps = h->Nk * (int)sizeof(double2) + 16;  // the plane and its load barrier
+        // the persistent plane kernel keeps the root and coordinate tables
+        // beside its plane when two CTAs still fit an SM
+        const size_t tb = tabs.roots.size() * sizeof(double2) + ((tabs.rpos.size() * sizeof(double) + 15) & ~(size_t)15);
+        if ((size_t)h->Nk * sizeof(double2) + tb <= 110 * 1024) {
+            h->nroot_s = (int)tabs.roots.size();
+            h->nrpos_s = (int)tabs.rpos.size();
+            h->tab_smem = (int)tb;
+        }
+    }
+    {
+        const int ps = h->Nk * (int)sizeof(double2) + 16 + h->tab_smem;  // the plane, its load barrier, the tables
         if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadix89, kPersist89Threads, kPersist89Batch>, ps))) return bail(rc);
         if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadix89, kPersist89Threads, kPersist89Batch>, ps))) return bail(rc);
         if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadixAll, 256>, ps))) return bail(rc);

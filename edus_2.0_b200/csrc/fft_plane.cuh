@@ -92,9 +92,10 @@ __device__ __forceinline__ C cmul_si(C a) {
     return S > 0 ? cmake<C>(-a.y, a.x) : cmake<C>(a.y, -a.x);
 }
 // root table entries are FP64; the FP32 transform rounds them once on use
+// (the table may sit in global or in shared memory)
 template <typename C>
 __device__ __forceinline__ C ldroot(const double2* p) {
-    const double2 w = __ldg(p);
+    const double2 w = *p;
     return cmake<C>((typename CplxT<C>::T)w.x, (typename CplxT<C>::T)w.y);
 }
 
@@ -230,14 +231,61 @@ struct Dft<11, S, C> : DftGeneric<11, S, C> {};
 template <int S, typename C>
 struct Dft<13, S, C> : DftGeneric<13, S, C> {};
 
+// cos(2 pi m / R) and sin(2 pi m / R) for the composite radices (R = 6, 9, 10,
+// 12; 0 < m < R, m not a quarter turn), as constants: m is a compile-time
+// value wherever these are called (unrolled loops), so the switch folds away.
+__device__ __forceinline__ double2 kcossin(int R, int m) {
+    const bool neg = 2 * m > R;  // sin(2 pi (R - m) / R) = -sin(2 pi m / R)
+    const int q = neg ? R - m : m;
+    double c = 0.0, s = 0.0;
+    if (R == 6 || (R == 12 && q == 2)) {  // 2 pi / 6
+        c = 0.5;
+        s = 0.86602540378443864676;
+    }
+    if ((R == 6 && q == 2) || (R == 9 && q == 3) || (R == 12 && q == 4)) {  // 2 pi / 3
+        c = -0.5;
+        s = 0.86602540378443864676;
+    }
+    if (R == 9) {
+        if (q == 1) { c = 0.76604444311897803520; s = 0.64278760968653932632; }
+        if (q == 2) { c = 0.17364817766693034885; s = 0.98480775301220805936; }
+        if (q == 4) { c = -0.93969262078590838405; s = 0.34202014332566873304; }
+    }
+    if (R == 10) {
+        if (q == 1) { c = 0.80901699437494742410; s = 0.58778525229247312917; }
+        if (q == 2) { c = 0.30901699437494742410; s = 0.95105651629515357212; }
+        if (q == 3) { c = -0.30901699437494742410; s = 0.95105651629515357212; }
+        if (q == 4) { c = -0.80901699437494742410; s = 0.58778525229247312917; }
+    }
+    if (R == 12) {
+        if (q == 1) { c = 0.86602540378443864676; s = 0.5; }
+        if (q == 5) { c = -0.86602540378443864676; s = 0.5; }
+    }
+    return make_double2(c, neg ? -s : s);
+}
+
+// u * exp(S 2 pi i m / R) for the composite radices' inner twiddles; quarter
+// turns are exact (a swap or a sign).
+template <int R, int S, typename C>
+__device__ __forceinline__ C kroot_mul(C u, int m) {
+    using T = typename CplxT<C>::T;
+    if ((4 * m) % R == 0) {
+        const int k = (4 * m / R) & 3;
+        if (k == 1) return cmul_si<S>(u);
+        if (k == 2) return cmake<C>(-u.x, -u.y);
+        return cmul_si<-S>(u);
+    }
+    const double2 w = kcossin(R, m);
+    return cmul(u, cmake<C>((T)w.x, (T)(S * w.y)));
+}
+
 // Composite radix R = R1*R2 entirely in registers (four-step):
 //   y[k1 + R1 k2] = sum_n2 W_R2^{n2 k2} W_R^{n2 k1} sum_n1 x[R2 n1 + n2] W_R1^{n1 k1}
-// with W_R^m = root[m * (n / R)] (conjugated for S = +1).
+// with W_R^m = exp(-2 pi i m / R) (conjugated for S = +1) from constants.
 template <int R1, int R2, int S, typename C>
 struct DftComposite {
     __device__ __forceinline__ static void run(C* v, const double2* root, int n) {
         constexpr int R = R1 * R2;
-        const int step = n / R;
         // phase 1, in place: v[R2 k1 + n2] <- W_R^{n2 k1} DFT_R1(v[R2 n1 + n2])_k1
 #pragma unroll
         for (int n2 = 0; n2 < R2; ++n2) {
@@ -247,13 +295,10 @@ struct DftComposite {
             Dft<R1, S, C>::run(u, root, n);
 #pragma unroll
             for (int k1 = 0; k1 < R1; ++k1) {
-                if (n2 * k1 == 0) {
+                if (n2 * k1 == 0)
                     v[R2 * k1 + n2] = u[k1];
-                } else {
-                    C w = ldroot<C>(&root[n2 * k1 * step]);
-                    if (S > 0) w.y = -w.y;
-                    v[R2 * k1 + n2] = cmul(u[k1], w);
-                }
+                else
+                    v[R2 * k1 + n2] = kroot_mul<R, S>(u[k1], n2 * k1);
             }
         }
         // phase 2, in place: v[R2 k1 + k2] <- DFT_R2(v[R2 k1 + n2])_k2

@@ -225,7 +225,8 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     const double2* __restrict__ roots, const double* __restrict__ rpos, PlanePlan pl, int nb, double inv_nk,
     double2* __restrict__ scratch, int nplanes, const int* __restrict__ hpos, const double2* __restrict__ hval,
     int nS, const int* __restrict__ opos, const double2* __restrict__ oval, int nO,
-    const double2* __restrict__ ptab = nullptr, int ntab = 0, int* status = nullptr, int wait_polls = 1 << 22) {
+    const double2* __restrict__ ptab = nullptr, int ntab = 0, int* status = nullptr, int wait_polls = 1 << 22,
+    int nroot_s = 0, int nrpos_s = 0) {
     extern __shared__ double2 smem[];
     const int Nk = pl.Nk;
     const int P = nb * nb;
@@ -241,12 +242,24 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
         mbar_init(lbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
+    // the transform roots and the R coordinates, when the host found room for
+    // them beside the plane (nroot_s > 0), are read from shared memory
+    const double2* rt = roots;
+    const double* rq = rpos;
+    if (nroot_s > 0) {
+        double2* sr = X + Nk + 1;
+        double* sq = (double*)(sr + nroot_s);
+        for (int i = threadIdx.x; i < nroot_s; i += blockDim.x) sr[i] = __ldg(&roots[i]);
+        for (int i = threadIdx.x; i < nrpos_s; i += blockDim.x) sq[i] = __ldg(&rpos[i]);
+        rt = sr;
+        rq = sq;
+    }
     __syncthreads();
     double2* slot = scratch + (long long)blockIdx.x * Nk;
     const int n1 = pl.ax[1].n, n2 = pl.ax[2].n;
-    const double* rp0 = rpos + pl.ax[0].rposoff;
-    const double* rp1 = rpos + pl.ax[1].rposoff;
-    const double* rp2 = rpos + pl.ax[2].rposoff;
+    const double* rp0 = rq + pl.ax[0].rposoff;
+    const double* rp1 = rq + pl.ax[1].rposoff;
+    const double* rp2 = rq + pl.ax[2].rposoff;
     for (int w = blockIdx.x; w < nplanes; w += gridDim.x) {
         // the solves of one band-pair plane run side by side: rho0 and W, which
         // they share, come from HBM once and from L2 for the others
@@ -261,7 +274,7 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 const double2* src = rho + (long long)b * batch_stride_in + (long long)p * Nk;
                 for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
                 __syncthreads();
-                plane_forward<1, MASK, double2, BT>(X, 0, pl, roots);
+                plane_forward<1, MASK, double2, BT>(X, 0, pl, rt);
                 const int n = p / nb, m = p - (p / nb) * nb;
                 if (n == m && threadIdx.x == 0) diag0[b * nb + n] = cscale(X[0], inv_nk);
                 __syncthreads();
@@ -274,7 +287,7 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 add_model_R(X, hpos, hval, nS, p, P, F, tb, &pl);
                 __syncthreads();
             }
-            plane_inverse<1, MASK, double2, BT>(X, 0, pl, roots);
+            plane_inverse<1, MASK, double2, BT>(X, 0, pl, rt);
             double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
             for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = X[i];
             __syncthreads();  // X is reloaded by the next plane
@@ -306,7 +319,7 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 return;
             }
         }
-        plane_forward<1, MASK, double2, BT>(X, 0, pl, roots);
+        plane_forward<1, MASK, double2, BT>(X, 0, pl, rt);
         const StageField F = field[b];
         const int n = p / nb, m = p - (p / nb) * nb;
         if (COUL && n == m && threadIdx.x == 0) diag0[b * nb + n] = cscale(X[0], inv_nk);
@@ -316,13 +329,13 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
             const int q2 = j - t * n2;
             const int q0 = fdiv(t, pl.fd_n1);
             const int q1 = t - q0 * n1;
-            const double dot = F.g[0] * __ldg(&rp0[q0]) + F.g[1] * __ldg(&rp1[q1]) + F.g[2] * __ldg(&rp2[q2]);
+            const double dot = F.g[0] * rp0[q0] + F.g[1] * rp1[q1] + F.g[2] * rp2[q2];
             const double2 r = cscale(X[j], inv_nk);
             if (COUL) slot[j] = r;
             X[j] = make_double2(-dot * r.y, dot * r.x);
         }
         __syncthreads();
-        plane_inverse<1, MASK, double2, BT>(X, 0, pl, roots);
+        plane_inverse<1, MASK, double2, BT>(X, 0, pl, rt);
         double2* gdst = G_out + (long long)b * batch_stride_out + (long long)p * Nk;
         if (!bulk) {
             for (int i = threadIdx.x; i < Nk; i += blockDim.x) gdst[i] = X[i];
@@ -348,7 +361,25 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
             } else {
                 const double2* r0p = rho0p + (long long)p * Nk;
                 const double* wp = Wp + (long long)p * Nk;
-                for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
+                // four positions per thread at once: their twelve global
+                // loads are in flight together
+                constexpr int U = 4;
+                const int T = blockDim.x;
+                int j = threadIdx.x;
+                for (; j + (U - 1) * T < Nk; j += U * T) {
+                    double2 r[U], r0[U];
+                    double wv[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        r[u] = slot[j + u * T];
+                        r0[u] = __ldg(&r0p[j + u * T]);
+                        wv[u] = __ldg(&wp[j + u * T]);
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        X[j + u * T] = make_double2(-wv[u] * (r[u].x - r0[u].x), -wv[u] * (r[u].y - r0[u].y));
+                }
+                for (; j < Nk; j += T) {
                     const double2 r = slot[j];
                     const double2 r0 = __ldg(&r0p[j]);
                     const double wv = __ldg(&wp[j]);
@@ -360,7 +391,7 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 add_model_R(X, hpos, hval, nS, p, P, F);
                 __syncthreads();
             }
-            plane_inverse<1, MASK, double2, BT>(X, 0, pl, roots);
+            plane_inverse<1, MASK, double2, BT>(X, 0, pl, rt);
             double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
             if (!bulk) {
                 for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = X[i];
