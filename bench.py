@@ -49,18 +49,64 @@ def workload_input(cache_dir: str) -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event reasons sampled during the timed region.
+
+    NVML read-only queries every 10 ms from a host thread (so that a timed
+    region of a few tens of milliseconds still holds several samples); the
+    nvidia-smi query loop at 200 ms where the NVML bindings are missing."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, interval_s: float = 0.01):
         self.dev = device_index
+        self.interval = interval_s
         self.proc = None
-        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.thread = None
+        self.rows = []  # (sm_mhz, sm_max_mhz, set of reasons)
+        self.error = ""
+
+    def _nvml_handle(self, nv):
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.dev)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _nvml_loop(self, nv, h, bits):
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.rows.append((float(sm), float(smax), {n for n, b in bits if r & b}))
+            self._stop.wait(self.interval)
 
     def __enter__(self):
+        import threading
+
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = self._nvml_handle(nv)
+            bits = [(n, getattr(nv, a)) for n, a in zip(self.NAMES, (
+                "nvmlClocksEventReasonHwSlowdown", "nvmlClocksEventReasonHwThermalSlowdown",
+                "nvmlClocksEventReasonSwThermalSlowdown", "nvmlClocksEventReasonSwPowerCap"))]
+            self._stop = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h, bits), daemon=True)
+            self.thread.start()
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 5.0:
+                time.sleep(0.002)
+            return self
+        except Exception as e:  # no NVML bindings or no device: nvidia-smi
+            self.error = f"nvml: {e}"[:120]
+            self.thread = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.err = tempfile.NamedTemporaryFile("w+", suffix=".err", delete=False)
         try:
             self.proc = subprocess.Popen(
@@ -79,6 +125,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self._stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -87,28 +136,32 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        self.out.flush()
-        rows = []
-        with open(self.out.name) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.out.name)
+        rows = list(self.rows)
+        source = "nvml 10 ms"
+        if self.thread is None:
+            source = "nvidia-smi 200 ms"
+            rows = []
+            if self.proc is not None:
+                self.out.flush()
+                with open(self.out.name) as f:
+                    for line in f:
+                        parts = [p.strip() for p in line.split(",")]
+                        if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                            rows.append((float(parts[1]), float(parts[2]) if parts[2].replace(".", "").isdigit()
+                                         else float("nan"),
+                                         {self.NAMES[i] for i in range(4) if parts[5 + i].lower() == "active"}))
+                os.unlink(self.out.name)
+                try:
+                    with open(self.err.name) as f:
+                        self.error = (self.error + " " + f.read().strip())[:200]
+                except OSError:
+                    pass
         if not rows:
-            err = ""
-            try:
-                with open(self.err.name) as f:
-                    err = f.read().strip()[:200]
-            except OSError:
-                pass
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0, "error": err}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0,
+                    "error": self.error.strip()}
+        return {"sm_mhz": float(np.median([r[0] for r in rows])),
+                "sm_max_mhz": float(np.nanmax([r[1] for r in rows])),
+                "reasons": sorted(set().union(*[r[2] for r in rows])), "samples": len(rows), "source": source}
 
 
 def measured_peaks():
