@@ -104,6 +104,7 @@ struct edus_handle {
     int split_grid = 0, split_threads = 256;
     PlaneLaunch plane_cfg{0, 512, false};
     int plane_grid = 0;            // persistent plane kernel: CTAs per launch
+    bool rows_ok = false;          // persistent plane kernel: row-wise variant (2-D grids)
     int nroot_s = 0, nrpos_s = 0;  // persistent plane kernel: root / coordinate entries it stages in shared memory
     int tab_smem = 0;              // their bytes (0: read from global memory)
     int wait_polls = 1 << 22;      // the plane kernel's bulk-load wait limit (edus_set_wait_limit)
@@ -343,8 +344,16 @@ void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long l
                           double2* Hee, long long out_bstride, const StageField* field, int nS,
                           const double2* ptab = nullptr) {
     const int grid = std::min(nplanes, h->plane_grid);
-    plane_rhs_persist_kernel<COUL, MASK, MAXT, BT>
-        <<<grid, h->plane_cfg.threads, h->Nk * sizeof(double2) + 16 + h->tab_smem, h->stream>>>(
+    const size_t smem = h->Nk * sizeof(double2) + 16 + h->tab_smem;
+    // 2-D grids in the length gauge: the row-wise kernel (warps own rows of
+    // the unit-stride axis; fewer CTA barriers, bitwise the same results)
+    if (h->rows_ok && !ptab)
+        plane_rhs_persist_kernel<COUL, MASK, MAXT, BT, true><<<grid, h->plane_cfg.threads, smem, h->stream>>>(
+            in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
+            1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0, ptab,
+            h->ntab, h->flag, h->wait_polls, h->nroot_s, h->nrpos_s);
+    else
+        plane_rhs_persist_kernel<COUL, MASK, MAXT, BT><<<grid, h->plane_cfg.threads, smem, h->stream>>>(
             in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
             1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0, ptab,
             h->ntab, h->flag, h->wait_polls, h->nroot_s, h->nrpos_s);
@@ -1185,6 +1194,14 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
         if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadixAll, 256>, ps))) return bail(rc);
         if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadixCommon, 256>, ps))) return bail(rc);
         if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadixCommon, 256>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadix89, kPersist89Threads, kPersist89Batch, true>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadix89, kPersist89Threads, kPersist89Batch, true>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadixAll, 256, 1, true>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadixAll, 256, 1, true>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadixCommon, 256, 1, true>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadixCommon, 256, 1, true>, ps))) return bail(rc);
+        // the row-wise variant: 2-D grids (unit-stride axis ax[1] with stages, several rows)
+        h->rows_ok = h->plan.ax[2].n == 1 && h->plan.ax[0].n > 1 && h->plan.ax[1].nst > 0;
     }
     if ((rc = set_smem(h, plane_rhs_kernel<true, kRadixAll, 512>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_rhs_kernel<false, kRadixAll, 512>, h->smem_plane))) return bail(rc);

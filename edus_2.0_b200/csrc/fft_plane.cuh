@@ -477,6 +477,104 @@ __device__ __forceinline__ void run_stage(C* buf, int bufstride, int Nk, const A
 #undef EDUS_STAGE_CASE
 }
 
+// Row-wise stages for 2-D planes (N2 = 1): the unit-stride axis ax[1] of
+// rows line0 .. line0 + nl - 1 (each n1 = ax[1].n consecutive elements) in
+// one warp, without a CTA barrier: the stages of that axis only touch the
+// elements of a row, so a warp that owns whole rows runs them, and the
+// pointwise steps between them, alone (__syncwarp between stages).  Lane l
+// takes the row-local butterflies l, l + 32, ... in the order of stage_R.
+template <int R, bool FWD>
+__device__ __forceinline__ void stage_R_rows(double2* X, const AxisPlan& ax, int s, const double2* __restrict__ root,
+                                             int line0, int nl) {
+    const int n = ax.n;
+    const int L = ax.L[s];
+    const int M = L * R;
+    const int nbfly = n / R;
+    const int tw_step = n / M;
+    const FastDiv fdb = ax.fd_nbfly[s], fdl = ax.fd_L[s];
+    const int lane = threadIdx.x & 31;
+    for (int i = lane; i < nl * nbfly; i += 32) {
+        const int li = fdiv(i, fdb);
+        const int bfly = i - li * nbfly;
+        const int blk = fdiv(bfly, fdl);
+        const int a = bfly - blk * L;
+        const int base = (line0 + li) * n + blk * M + a;
+        double2 v[R];
+#pragma unroll
+        for (int b = 0; b < R; ++b) v[b] = X[base + b * L];
+        butterfly_R<R, FWD, double2>(v, a, tw_step, n, root);
+#pragma unroll
+        for (int b = 0; b < R; ++b) X[base + b * L] = v[b];
+    }
+}
+
+template <bool FWD, int MASK>
+__device__ __forceinline__ void run_stage_rows(double2* X, const AxisPlan& ax, int s, const double2* __restrict__ roots,
+                                               int line0, int nl) {
+    const double2* root = roots + ax.rootoff;
+    const int r = ax.r[s];
+#define EDUS_ROWS_CASE(R)                                            \
+    if constexpr ((MASK >> R) & 1) {                                 \
+        if (r == R) {                                                \
+            stage_R_rows<R, FWD>(X, ax, s, root, line0, nl);         \
+            return;                                                  \
+        }                                                            \
+    }
+    EDUS_ROWS_CASE(2)
+    EDUS_ROWS_CASE(3)
+    EDUS_ROWS_CASE(4)
+    EDUS_ROWS_CASE(5)
+    EDUS_ROWS_CASE(6)
+    EDUS_ROWS_CASE(7)
+    EDUS_ROWS_CASE(8)
+    EDUS_ROWS_CASE(9)
+    EDUS_ROWS_CASE(10)
+    EDUS_ROWS_CASE(11)
+    EDUS_ROWS_CASE(12)
+    EDUS_ROWS_CASE(13)
+#undef EDUS_ROWS_CASE
+}
+
+// The ax[1] part of plane_forward (FWD) or plane_inverse for the warp's rows.
+template <bool FWD, int MASK>
+__device__ __forceinline__ void rows_transform(double2* X, const PlanePlan& pl, const double2* __restrict__ roots,
+                                               int line0, int nl) {
+    const AxisPlan& ax = pl.ax[1];
+    if (FWD) {
+#pragma unroll 1
+        for (int s = 0; s < ax.nst; ++s) {
+            run_stage_rows<true, MASK>(X, ax, s, roots, line0, nl);
+            __syncwarp();
+        }
+    } else {
+#pragma unroll 1
+        for (int s = ax.nst - 1; s >= 0; --s) {
+            run_stage_rows<false, MASK>(X, ax, s, roots, line0, nl);
+            __syncwarp();
+        }
+    }
+}
+
+// The ax[0] part of plane_forward (FWD) or plane_inverse, CTA-wide, each stage
+// followed by a CTA barrier.
+template <bool FWD, int MASK>
+__device__ __forceinline__ void axis0_transform(double2* X, const PlanePlan& pl, const double2* __restrict__ roots) {
+    const AxisPlan& ax = pl.ax[0];
+    if (FWD) {
+#pragma unroll 1
+        for (int s = 0; s < ax.nst; ++s) {
+            run_stage<true, 1, MASK, double2>(X, 0, pl.Nk, ax, s, roots);
+            __syncthreads();
+        }
+    } else {
+#pragma unroll 1
+        for (int s = ax.nst - 1; s >= 0; --s) {
+            run_stage<false, 1, MASK, double2>(X, 0, pl.Nk, ax, s, roots);
+            __syncthreads();
+        }
+    }
+}
+
 // Forward (k -> R, unnormalised sign -1) transform of the plane(s) in place.
 template <int NBUF, int MASK, typename C, int BT = 1>
 __device__ __forceinline__ void plane_forward(C* buf, int bufstride, const PlanePlan& pl, const double2* __restrict__ roots) {

@@ -217,7 +217,14 @@ __global__ void __launch_bounds__(MAXT) plane_rhs_kernel(
 // inverse transforms run in turn from one buffer; rho(R) survives the first
 // in the CTA's own slot of `scratch` ([gridDim.x][Nk], written and read back
 // by the same thread, so it stays in L2 and needs no fence).
-template <bool COUL, int MASK, int MAXT, int BT = 1>
+//
+// ROWS (2-D grids, N2 = 1, length gauge): warp w owns rows [w lpw, (w+1) lpw)
+// of the unit-stride axis ax[1] and runs that axis's stages, the gradient's
+// pointwise step, the self-energy pass and the model terms on them alone;
+// only the ax[0] stages, which mix rows, are CTA-wide.  The arithmetic is the
+// same as without ROWS, in the same order, so the results are bitwise equal;
+// a plane then needs 9 CTA barriers instead of 16.
+template <bool COUL, int MASK, int MAXT, int BT = 1, bool ROWS = false>
 __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     const double2* __restrict__ rho, long long batch_stride_in, double2* __restrict__ G_out,
     double2* __restrict__ Hee_out, long long batch_stride_out, const double2* __restrict__ rho0p,
@@ -260,12 +267,17 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     const double* rp0 = rq + pl.ax[0].rposoff;
     const double* rp1 = rq + pl.ax[1].rposoff;
     const double* rp2 = rq + pl.ax[2].rposoff;
+    // ROWS: this warp's rows of the unit-stride axis
+    const int lane = threadIdx.x & 31;
+    const int lpw = (pl.ax[0].n + (int)(blockDim.x >> 5) - 1) / (int)(blockDim.x >> 5);
+    const int line0 = (int)(threadIdx.x >> 5) * lpw;
+    const int nl = max(0, min(lpw, pl.ax[0].n - line0));
     for (int w = blockIdx.x; w < nplanes; w += gridDim.x) {
         // the solves of one band-pair plane run side by side: rho0 and W, which
         // they share, come from HBM once and from L2 for the others
         const int nbat = nplanes / P;
         const int p = w / nbat, b = w - (w / nbat) * nbat;
-        if (ptab) {
+        if (!ROWS && ptab) {
             // Peierls gauge: no gradient term, two transforms (one without
             // HSEX); H = (H0 + E.xi + Hee[rho e^{-iA.R}]) e^{iA.R}
             const double2* tb = ptab + (long long)b * ntab;
@@ -319,23 +331,48 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 return;
             }
         }
-        plane_forward<1, MASK, double2, BT>(X, 0, pl, rt);
         const StageField F = field[b];
-        const int n = p / nb, m = p - (p / nb) * nb;
-        if (COUL && n == m && threadIdx.x == 0) diag0[b * nb + n] = cscale(X[0], inv_nk);
-        __syncthreads();
-        for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
-            const int t = fdiv(j, pl.fd_n2);
-            const int q2 = j - t * n2;
-            const int q0 = fdiv(t, pl.fd_n1);
-            const int q1 = t - q0 * n1;
-            const double dot = F.g[0] * rp0[q0] + F.g[1] * rp1[q1] + F.g[2] * rp2[q2];
-            const double2 r = cscale(X[j], inv_nk);
-            if (COUL) slot[j] = r;
-            X[j] = make_double2(-dot * r.y, dot * r.x);
+        if constexpr (ROWS) {
+            axis0_transform<true, MASK>(X, pl, rt);
+            rows_transform<true, MASK>(X, pl, rt, line0, nl);
+            const int n = p / nb, m = p - (p / nb) * nb;
+            double2* const dg = (COUL && n == m) ? diag0 + b * nb + n : nullptr;
+            const double g2 = F.g[2] * rp2[0];
+            for (int idx = lane; idx < nl * n1; idx += 32) {
+                const int li = fdiv(idx, pl.fd_n1);
+                const int q1 = idx - li * n1;
+                const int q0 = line0 + li;
+                const int j = q0 * n1 + q1;
+                const double dot = F.g[0] * rp0[q0] + F.g[1] * rp1[q1] + g2;
+                const double2 r = cscale(X[j], inv_nk);
+                if (COUL) {
+                    slot[j] = r;
+                    if (j == 0 && dg) *dg = r;
+                }
+                X[j] = make_double2(-dot * r.y, dot * r.x);
+            }
+            __syncwarp();
+            rows_transform<false, MASK>(X, pl, rt, line0, nl);
+            __syncthreads();
+            axis0_transform<false, MASK>(X, pl, rt);
+        } else {
+            plane_forward<1, MASK, double2, BT>(X, 0, pl, rt);
+            const int n = p / nb, m = p - (p / nb) * nb;
+            if (COUL && n == m && threadIdx.x == 0) diag0[b * nb + n] = cscale(X[0], inv_nk);
+            __syncthreads();
+            for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
+                const int t = fdiv(j, pl.fd_n2);
+                const int q2 = j - t * n2;
+                const int q0 = fdiv(t, pl.fd_n1);
+                const int q1 = t - q0 * n1;
+                const double dot = F.g[0] * rp0[q0] + F.g[1] * rp1[q1] + F.g[2] * rp2[q2];
+                const double2 r = cscale(X[j], inv_nk);
+                if (COUL) slot[j] = r;
+                X[j] = make_double2(-dot * r.y, dot * r.x);
+            }
+            __syncthreads();
+            plane_inverse<1, MASK, double2, BT>(X, 0, pl, rt);
         }
-        __syncthreads();
-        plane_inverse<1, MASK, double2, BT>(X, 0, pl, rt);
         double2* gdst = G_out + (long long)b * batch_stride_out + (long long)p * Nk;
         if (!bulk) {
             for (int i = threadIdx.x; i < Nk; i += blockDim.x) gdst[i] = X[i];
@@ -362,11 +399,12 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 const double2* r0p = rho0p + (long long)p * Nk;
                 const double* wp = Wp + (long long)p * Nk;
                 // four positions per thread at once: their twelve global
-                // loads are in flight together
+                // loads are in flight together (ROWS: the warp's rows)
                 constexpr int U = 4;
-                const int T = blockDim.x;
-                int j = threadIdx.x;
-                for (; j + (U - 1) * T < Nk; j += U * T) {
+                const int T = ROWS ? 32 : (int)blockDim.x;
+                const int jend = ROWS ? (line0 + nl) * n1 : Nk;
+                int j = ROWS ? line0 * n1 + lane : (int)threadIdx.x;
+                for (; j + (U - 1) * T < jend; j += U * T) {
                     double2 r[U], r0[U];
                     double wv[U];
 #pragma unroll
@@ -379,19 +417,46 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                     for (int u = 0; u < U; ++u)
                         X[j + u * T] = make_double2(-wv[u] * (r[u].x - r0[u].x), -wv[u] * (r[u].y - r0[u].y));
                 }
-                for (; j < Nk; j += T) {
+                for (; j < jend; j += T) {
                     const double2 r = slot[j];
                     const double2 r0 = __ldg(&r0p[j]);
                     const double wv = __ldg(&wp[j]);
                     X[j] = make_double2(-wv * (r.x - r0.x), -wv * (r.y - r0.y));
                 }
             }
-            __syncthreads();
-            if (nS > 0) {
-                add_model_R(X, hpos, hval, nS, p, P, F);
+            if constexpr (ROWS) {
+                if (nO > 0) __syncthreads();  // the CTA-wide scatter above is complete
+                __syncwarp();                 // the warp's own self-energy stores
+                // the model terms on this warp's rows (add_model_R restricted to them)
+                for (int s2 = lane; s2 < nS; s2 += 32) {
+                    const int pos = __ldg(&hpos[s2]);
+                    if ((unsigned)(fdiv(pos, pl.fd_n1) - line0) >= (unsigned)nl) continue;
+                    double2 mv = __ldg(&hval[(long long)p * nS + s2]);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        if (F.E[d] != 0.0) {
+                            const double2 x = __ldg(&hval[((long long)(d + 1) * P + p) * nS + s2]);
+                            mv.x += F.E[d] * x.x;
+                            mv.y += F.E[d] * x.y;
+                        }
+                    }
+                    double2 v = X[pos];
+                    v.x += mv.x;
+                    v.y += mv.y;
+                    X[pos] = v;
+                }
+                __syncwarp();
+                rows_transform<false, MASK>(X, pl, rt, line0, nl);
                 __syncthreads();
+                axis0_transform<false, MASK>(X, pl, rt);
+            } else {
+                __syncthreads();
+                if (nS > 0) {
+                    add_model_R(X, hpos, hval, nS, p, P, F);
+                    __syncthreads();
+                }
+                plane_inverse<1, MASK, double2, BT>(X, 0, pl, rt);
             }
-            plane_inverse<1, MASK, double2, BT>(X, 0, pl, rt);
             double2* hdst = Hee_out + (long long)b * batch_stride_out + (long long)p * Nk;
             if (!bulk) {
                 for (int i = threadIdx.x; i < Nk; i += blockDim.x) hdst[i] = X[i];
