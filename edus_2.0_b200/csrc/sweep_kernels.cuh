@@ -64,23 +64,48 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 2 : 1) sweep_plane_kernel(
         const double2* src = a.rho + off;
         for (int i = threadIdx.x; i < Nk; i += blockDim.x) X[i] = __ldg(&src[i]);
         __syncthreads();
-        plane_forward<1, MASK>(X, 0, pl, d.roots);
         const StageField F = a.field[it.y];
         const int n1 = pl.ax[1].n, n2 = pl.ax[2].n;
         const double* rp0 = d.rpos + pl.ax[0].rposoff;
         const double* rp1 = d.rpos + pl.ax[1].rposoff;
         const double* rp2 = d.rpos + pl.ax[2].rposoff;
-        for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
-            const int t = fdiv(j, pl.fd_n2);
-            const int q2 = j - t * n2;
-            const int q0 = fdiv(t, pl.fd_n1);
-            const int q1 = t - q0 * n1;
-            const double dot = F.g[0] * __ldg(&rp0[q0]) + F.g[1] * __ldg(&rp1[q1]) + F.g[2] * __ldg(&rp2[q2]);
-            const double2 r = cscale(X[j], d.inv_nk);
-            X[j] = make_double2(-dot * r.y, dot * r.x);
+        if (n2 == 1 && pl.ax[0].n > 1 && pl.ax[1].nst > 0) {
+            // 2-D plane: row-wise, as plane_rhs_persist_kernel<..., ROWS>
+            // (warps own rows of the unit-stride axis; the same arithmetic)
+            const int nw = (int)(blockDim.x >> 5);
+            const int lpw = (pl.ax[0].n + nw - 1) / nw;
+            const int line0 = (int)(threadIdx.x >> 5) * lpw;
+            const int nl = max(0, min(lpw, pl.ax[0].n - line0));
+            axis0_transform<true, MASK>(X, pl, d.roots);
+            rows_transform<true, MASK>(X, pl, d.roots, line0, nl);
+            for (int idx = (int)(threadIdx.x & 31); idx < nl * n1; idx += 32) {
+                const int li = fdiv(idx, pl.fd_n1);
+                const int q1 = idx - li * n1;
+                const int q0 = line0 + li;
+                const int j = q0 * n1 + q1;
+                const double dot = F.g[0] * __ldg(&rp0[q0]) + F.g[1] * __ldg(&rp1[q1]) + F.g[2] * __ldg(&rp2[0]);
+                const double2 r = cscale(X[j], d.inv_nk);
+                X[j] = make_double2(-dot * r.y, dot * r.x);
+            }
+            __syncwarp();
+            rows_transform<false, MASK>(X, pl, d.roots, line0, nl);
+            __syncthreads();
+            axis0_transform<false, MASK>(X, pl, d.roots);
+        } else {
+            plane_forward<1, MASK>(X, 0, pl, d.roots);
+            for (int j = threadIdx.x; j < Nk; j += blockDim.x) {
+                const int t = fdiv(j, pl.fd_n2);
+                const int q2 = j - t * n2;
+                const int q0 = fdiv(t, pl.fd_n1);
+                const int q1 = t - q0 * n1;
+                const double dot =
+                    F.g[0] * __ldg(&rp0[q0]) + F.g[1] * __ldg(&rp1[q1]) + F.g[2] * __ldg(&rp2[q2]);
+                const double2 r = cscale(X[j], d.inv_nk);
+                X[j] = make_double2(-dot * r.y, dot * r.x);
+            }
+            __syncthreads();
+            plane_inverse<1, MASK>(X, 0, pl, d.roots);
         }
-        __syncthreads();
-        plane_inverse<1, MASK>(X, 0, pl, d.roots);
         double2* dst = d.G + off;
         for (int i = threadIdx.x; i < Nk; i += blockDim.x) dst[i] = X[i];
     }
