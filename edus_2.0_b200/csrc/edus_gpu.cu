@@ -2253,11 +2253,22 @@ static int fused_launch_steps(edus_handle* const* hs, const FusedSweep& f, int c
 
 extern "C" {
 
+// States up to this size step through CUDA graphs when a call covers enough
+// steps (edus_step): their steps take tens of microseconds, of which the
+// launches are a large part.
+constexpr size_t kGraphStepBytes = 16u << 20;
+constexpr int kGraphStepMin = 128;
+
 int edus_step(edus_handle* h, int n) {
     if (!h || n < 0) return EDUS_ERR_ARG;
     if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "edus_upload_model must be called first");
     CU(h, cudaSetDevice(h->d.device));
     const bool rk = h->d.solver == EDUS_SOLVER_RK;
+    // small RK4 problems in the FP64 form: the same launches, 32 steps per
+    // CUDA graph replay (captured once per call)
+    if (rk && !h->packed && !h->split && !h->profiling && n >= kGraphStepMin &&
+        (size_t)h->S * h->B * sizeof(double2) <= kGraphStepBytes)
+        return edus_sweep_step(&h, 1, n, 1);
     const int nst = rk ? 4 : 1;
     const double dt = h->d.dt;
     const int B = h->B;
