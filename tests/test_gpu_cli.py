@@ -5,8 +5,9 @@
   reference's outputs at ci-test/compare.py's 1e-10 (Time.txt is printed with
   6 significant digits);
 * cli.run on every case of tests/golden/ref_cases.py (HSEX, RK4 / AB4 / AB5,
-  even and odd grids, 2 to 13 bands, the k-space gradient, the Peierls gauge)
-  writes Population.txt, Population_wannier.txt and Velocity.txt that match the
+  even and odd grids, 2 to 22 bands, the k-space gradient, the Peierls gauge,
+  and the benchmark's own 22-orbital 72 x 72 HSEX model at full size) writes
+  Population.txt, Population_wannier.txt and Velocity.txt that match the
   outputs of the reference's own propagator (tests/golden/ref/) at 1e-10;
 * edus_observables equals the populations and velocity computed on the host
   from the state, the eigenvectors and the velocity operator.
@@ -84,6 +85,27 @@ def test_cli_reproduces_reference_outputs(pkg, tmp_path, name):
         assert got.shape == ref.shape, fn
         err = np.abs(got - ref).max()
         assert err < 1e-10, f"{name} {fn}: max |GPU - reference| = {err:.3e}"
+
+
+def test_full_size_case_has_teeth(pkg, tmp_path):
+    """The benchmark model at full size (tmd22_72_rk4): without the HSEX term the
+    same run misses the reference's populations by far more than the 1e-10 the
+    product holds, so that case pins the self-energy the benchmark runs."""
+    rc = _ref_cases()
+    case = dict(rc.CASES["tmd22_72_rk4"])
+    seed = rc.write_model(pkg.workloads, case, str(tmp_path))
+    inp = rc.make_input(case, seed)
+    inp["coulomb"] = False
+    path = os.path.join(str(tmp_path), "input.json")
+    with open(path, "w") as f:
+        json.dump(inp, f)
+    out = os.path.join(str(tmp_path), "Output")
+    from edus_b200 import cli
+
+    cli.run(path, out)
+    got = np.loadtxt(os.path.join(out, "Population.txt"))
+    ref = np.loadtxt(os.path.join(GOLDEN, "ref", "tmd22_72_rk4", "Population.txt"))
+    assert np.abs(got - ref).max() > 1e-7
 
 
 def test_observables_match_host(pkg, tmp_path):

@@ -52,7 +52,12 @@ def _load(name, fn):
     return a
 
 
-@pytest.mark.parametrize("name", sorted(ref_cases.CASES))
+# cases sized for the GPU only (the benchmark model at full size) are left to
+# tests/test_gpu_cli.py: the CPU oracle would take minutes on them
+CPU_CASES = sorted(n for n, c in ref_cases.CASES.items() if not c.get("gpu_only"))
+
+
+@pytest.mark.parametrize("name", CPU_CASES)
 def test_oracle_matches_reference(po, pkg, tmp_path, name):
     case = ref_cases.CASES[name]
     meta = json.load(open(os.path.join(REF, name, "meta.json")))
@@ -72,7 +77,7 @@ def test_oracle_matches_reference(po, pkg, tmp_path, name):
     assert np.allclose(got["Time.txt"], t, rtol=1e-5, atol=1e-12)
 
 
-@pytest.mark.parametrize("name", sorted(n for n, c in ref_cases.CASES.items() if c["coulomb"]))
+@pytest.mark.parametrize("name", [n for n in CPU_CASES if ref_cases.CASES[n]["coulomb"]])
 def test_reference_outputs_depend_on_hsex(po, pkg, tmp_path, name):
     """The pin has teeth: the same run without the HSEX term misses the
     reference's populations by far more than the tolerance."""
