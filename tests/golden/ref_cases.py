@@ -57,6 +57,14 @@ CASES = {
     "tmd22_72_rk4": dict(model=("tmd22",), grid=(72, 72, 1), filled=11, dt=0.005, nsteps=40, solver="RK",
                          order=4, laser=(2.5, 5e13, 1, -0.827, (1, 0.5, 0)), coulomb=True, epsilon=1.0,
                          r0=40.0, gpu_only=True),
+    # the same model with the stepper of that configuration, Adams-Bashforth 4
+    # (cold history), 80 steps, at 2e12 W/cm2: the gradient term's largest rate,
+    # E R_max ~ E 216 bohr, times dt must stay inside AB4's stability interval
+    # on the imaginary axis (the 5e13 W/cm2 pulse above makes the reference's
+    # own AB4 run diverge after 40 steps)
+    "tmd22_72_ab4": dict(model=("tmd22",), grid=(72, 72, 1), filled=11, dt=0.005, nsteps=80, solver="AB",
+                         order=4, laser=(2.5, 2e12, 1, -0.827, (1, 0.5, 0)), coulomb=True, epsilon=1.0,
+                         r0=40.0, gpu_only=True),
 }
 
 OUTPUTS = ("Population.txt", "Population_wannier.txt", "Velocity.txt", "Laser.txt", "Time.txt")
