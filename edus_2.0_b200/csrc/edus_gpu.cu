@@ -2257,7 +2257,7 @@ extern "C" {
 // steps (edus_step): their steps take tens of microseconds, of which the
 // launches are a large part.
 constexpr size_t kGraphStepBytes = 16u << 20;
-constexpr int kGraphStepMin = 128;
+constexpr int kGraphStepMin = 512;
 
 int edus_step(edus_handle* h, int n) {
     if (!h || n < 0) return EDUS_ERR_ARG;

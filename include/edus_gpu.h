@@ -171,7 +171,7 @@ int edus_rhs(edus_handle* h, double t, const double* in_k, double* out_k);
 /* Advance every solve by n steps (DESolver::Propagate(n), DESolver.hpp:238-242).
  * Asynchronous: returns once the work is queued.  Exception: an RK4 handle in
  * the FP64 form whose state (all solves) is at most 16 MB, profiling off, with
- * n >= 128, steps as edus_sweep_step of that one handle with use_graph 1 (the
+ * n >= 512, steps as edus_sweep_step of that one handle with use_graph 1 (the
  * same launches, 32 steps per CUDA graph replay, for small problems whose
  * steps are dominated by launch overhead) and returns once they are done. */
 int edus_step(edus_handle* h, int n);
