@@ -150,12 +150,18 @@ class ClockSampler:
                             rows.append((float(parts[1]), float(parts[2]) if parts[2].replace(".", "").isdigit()
                                          else float("nan"),
                                          {self.NAMES[i] for i in range(4) if parts[5 + i].lower() == "active"}))
-                os.unlink(self.out.name)
                 try:
                     with open(self.err.name) as f:
                         self.error = (self.error + " " + f.read().strip())[:200]
                 except OSError:
                     pass
+            for tf in (getattr(self, "out", None), getattr(self, "err", None)):
+                if tf is not None:
+                    tf.close()
+                    try:
+                        os.unlink(tf.name)
+                    except OSError:
+                        pass
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0,
                     "error": self.error.strip()}
