@@ -195,7 +195,7 @@ def algorithmic_bytes(P, Nk, B, d_E, coulomb=True):
     return plane, comm
 
 
-FORMS = (("split32", "PREC_SPLIT32"), ("mixed", "PREC_MIXED"), ("herm64", "PREC_HERM64"))
+FORMS = (("split32", "PREC_SPLIT32"), ("mixed", "PREC_MIXED"), ("herm64", "PREC_HERM64"), ("hplanes", "PREC_HPLANES"))
 
 
 def _trajectory(s, b, vel, nsteps, every, filled):
@@ -269,7 +269,7 @@ def run_ours(args, rank, world, local_rank):
 
     pkg = ge.load_package()
     torch.cuda.set_device(local_rank)
-    cache = os.environ.get("EDUS_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "edus_bench_tmd22"))
+    cache = os.environ.get("EDUS_BENCH_CACHE", os.path.join(tempfile.gettempdir(), f"edus_bench_tmd22_{GRID[0]}x{GRID[1]}"))
     if world > 1:
         # one rank writes the model; the others wait for it
         if rank == 0:
@@ -428,7 +428,7 @@ def run_ours(args, rank, world, local_rank):
         "max_abs_drho": forms["batched_fp64"]["max_abs_drho"] if forms else None,
         "hhg_rel_err": forms["batched_fp64"]["hhg_rel_err"] if forms else None,
         "forms": forms,
-        "config": {"workload": f"{WORKLOAD}: 22-orbital TMD-like, 72x72x1 k grid, HSEX (RK r0=40 A, eps=1), "
+        "config": {"workload": f"{WORKLOAD}: 22-orbital TMD-like, {GRID[0]}x{GRID[1]}x1 k grid, HSEX (RK r0=40 A, eps=1), "
                                f"RK4 dt=0.005 fs, batch={B} solve(s) per GPU (laser intensity x(1 + b/4))",
                    "batch": B, "l2": f"inputs larger than L2 (state {S_bytes / 1e6:.1f} MB x {B}; "
                                      f"per-step traffic {step_B / 1e9:.2f} GB)",
@@ -516,7 +516,7 @@ def cpu_baseline(inp, steps=20, threads=None):
     if os.path.exists(REF_EXE):
         v, dt = reference_rate(inp, steps, 1, threads)
         return {"value": round(v, 5), "unit": "steps/s", "cores": threads, "kind": "reference",
-                "sample": f"{steps} RK4 steps of the full {WORKLOAD} workload (72x72, nb=22, HSEX) after 1 "
+                "sample": f"{steps} RK4 steps of the full {WORKLOAD} workload ({GRID[0]}x{GRID[1]}, nb=22, HSEX) after 1 "
                           f"warm-up step, {dt:.1f} s by the reference's Simulation::Propagate timer; reference "
                           f"sources with the project's MPI/FFTW/MKL stand-ins, OpenMP {threads} threads"}
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -532,13 +532,13 @@ def cpu_baseline(inp, steps=20, threads=None):
     o.step(steps)
     dt = time.perf_counter() - t
     return {"value": round(steps / dt, 5), "unit": "steps/s", "cores": threads, "kind": "port",
-            "sample": f"{steps} RK4 steps of the full {WORKLOAD} workload (72x72, nb=22, HSEX), "
+            "sample": f"{steps} RK4 steps of the full {WORKLOAD} workload ({GRID[0]}x{GRID[1]}, nb=22, HSEX), "
                       f"{dt:.1f} s, OpenMP {threads} threads (oracle/_ref/EDUS not built)"}
 
 
 def run_reference(args):
     """--impl reference: the reference's CPU propagation on the host cores."""
-    cache = os.environ.get("EDUS_BENCH_CACHE", os.path.join(tempfile.gettempdir(), "edus_bench_tmd22"))
+    cache = os.environ.get("EDUS_BENCH_CACHE", os.path.join(tempfile.gettempdir(), f"edus_bench_tmd22_{GRID[0]}x{GRID[1]}"))
     inp = workload_input(cache)
     threads = os.cpu_count()
     K = max(1, min(args.steps, args.ref_max_steps))
@@ -570,7 +570,7 @@ def run_reference(args):
         "metric": METRIC, "impl": "reference", "value": round(v, 5), "unit": "steps/s", "n_gpus": 0,
         "steps": K, "warmup": W, "ms_per_step": round(dt / K * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{WORKLOAD}: 22-orbital TMD-like, 72x72x1 k grid, HSEX, RK4 dt=0.005 fs",
+        "config": {"workload": f"{WORKLOAD}: 22-orbital TMD-like, {GRID[0]}x{GRID[1]}x1 k grid, HSEX, RK4 dt=0.005 fs",
                    "parallelism": "host cores"},
         "cpu_baseline": {"value": round(v, 5), "unit": "steps/s", "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": round(v, 5), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -794,6 +794,7 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--accuracy-steps", type=int, default=4000)
     ap.add_argument("--workload", choices=["tmd22_rk4", "sweep", "surrogate"], default="tmd22_rk4")
+    ap.add_argument("--grid", type=int, default=72, help="tmd22_rk4: N for the N x N k grid (72: the benchmark)")
     ap.add_argument("--surrogate-snapshots", type=int, default=2000)
     ap.add_argument("--surrogate-run-steps", type=int, default=2000)
     ap.add_argument("--surrogate-iters", type=int, default=3000)
@@ -801,6 +802,10 @@ def main():
     ap.add_argument("--solves", type=int, default=256)
     ap.add_argument("--no-autotune", action="store_true", help="sweep: keep the default launch variants")
     args = ap.parse_args()
+    global GRID, METRIC
+    if args.grid != 72:
+        GRID = (args.grid, args.grid, 1)
+        METRIC = METRIC.replace("72x72", f"{args.grid}x{args.grid}")
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     rank = int(os.environ.get("RANK", "0"))

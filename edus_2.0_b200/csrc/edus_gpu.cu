@@ -105,6 +105,9 @@ struct edus_handle {
     PlaneLaunch plane_cfg{0, 512, false};
     int plane_grid = 0;            // persistent plane kernel: CTAs per launch
     bool rows_ok = false;          // persistent plane kernel: row-wise variant (2-D grids)
+    bool hplanes = false;          // EDUS_PREC_HPLANES: pairs n <= m transformed, (m, n) conjugated
+    int Pu = 0;                    // nb (nb + 1) / 2
+    int* upair = nullptr;          // [Pu] n nb + m of the pairs n <= m
     int nroot_s = 0, nrpos_s = 0;  // persistent plane kernel: root / coordinate entries it stages in shared memory
     int tab_smem = 0;              // their bytes (0: read from global memory)
     int wait_polls = 1 << 22;      // the plane kernel's bulk-load wait limit (edus_set_wait_limit)
@@ -347,7 +350,12 @@ void launch_plane_persist(edus_handle* h, int nplanes, const double2* in, long l
     const size_t smem = h->Nk * sizeof(double2) + 16 + h->tab_smem;
     // 2-D grids in the length gauge: the row-wise kernel (warps own rows of
     // the unit-stride axis; fewer CTA barriers, bitwise the same results)
-    if (h->rows_ok && !ptab)
+    if (h->hplanes)
+        plane_rhs_persist_kernel<COUL, MASK, MAXT, BT, true, true><<<grid, h->plane_cfg.threads, smem, h->stream>>>(
+            in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
+            1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0, ptab,
+            h->ntab, h->flag, h->wait_polls, h->nroot_s, h->nrpos_s, h->upair);
+    else if (h->rows_ok && !ptab)
         plane_rhs_persist_kernel<COUL, MASK, MAXT, BT, true><<<grid, h->plane_cfg.threads, smem, h->stream>>>(
             in, in_bstride, G, Hee, out_bstride, h->rho0p, h->Wp, h->diag0, field, h->roots, h->rpos, h->plan, h->nb,
             1.0 / h->Nk, h->plane_scratch, nplanes, h->hpos, h->hval, nS, h->opos, h->oval, COUL ? h->nO : 0, ptab,
@@ -498,7 +506,7 @@ int launch_plane(edus_handle* h, const double2* in, long long in_bstride, double
         return EDUS_OK;
     }
     if (h->plane_cfg.persist) {
-        const int np = h->P * nbatch;
+        const int np = (h->hplanes ? h->Pu : h->P) * nbatch;
         if (h->plane_cfg.variant == 1) {
             if (c) launch_plane_persist<true, kRadix89, kPersist89Threads, kPersist89Batch>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
             else launch_plane_persist<false, kRadix89, kPersist89Threads, kPersist89Batch>(h, np, in, in_bstride, G, Hee, out_bstride, field, nS);
@@ -1104,9 +1112,10 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     if (d.solver == EDUS_SOLVER_AB && d.order != 4 && d.order != 5)
         return fail(nullptr, EDUS_ERR_UNSUPPORTED, "order not implemented for AB (DESolver.hpp:120-124)");
     if (d.precision != EDUS_PREC_FP64 && d.precision != EDUS_PREC_HERM64 && d.precision != EDUS_PREC_MIXED &&
-        d.precision != EDUS_PREC_SPLIT32)
+        d.precision != EDUS_PREC_SPLIT32 && d.precision != EDUS_PREC_HPLANES)
         return fail(nullptr, EDUS_ERR_UNSUPPORTED, "precision not supported");
     const bool packed_form = d.precision == EDUS_PREC_HERM64 || d.precision == EDUS_PREC_MIXED;
+    const bool herm_planes = d.precision == EDUS_PREC_HPLANES;
     if (packed_form && d.nbands > 32)
         return fail(nullptr, EDUS_ERR_UNSUPPORTED, "the packed-Hermitian forms handle up to 32 bands");
     if (d.batch < 1) return fail(nullptr, EDUS_ERR_ARG, "batch must be >= 1");
@@ -1143,8 +1152,8 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     }
     const std::vector<double2>& roots = tabs.roots;
     std::vector<double>& rpos = tabs.rpos;
-    if (packed_form) {
-        // The packed forms propagate the Hermitian part of the generator: on an
+    if (packed_form || herm_planes) {
+        // The Hermitian forms propagate the Hermitian part of the generator: on an
         // even axis the Gamma-centred index N/2 is -N/2 for both R and -R, so
         // the gradient's i (R.E) is not anti-Hermitian there; its Hermitian
         // part has coordinate 0 on that index.
@@ -1200,8 +1209,18 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
         if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadixAll, 256, 1, true>, ps))) return bail(rc);
         if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadixCommon, 256, 1, true>, ps))) return bail(rc);
         if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadixCommon, 256, 1, true>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadix89, kPersist89Threads, kPersist89Batch, true, true>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadix89, kPersist89Threads, kPersist89Batch, true, true>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadixAll, 256, 1, true, true>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadixAll, 256, 1, true, true>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<true, kRadixCommon, 256, 1, true, true>, ps))) return bail(rc);
+        if ((rc = set_smem(h, plane_rhs_persist_kernel<false, kRadixCommon, 256, 1, true, true>, ps))) return bail(rc);
         // the row-wise variant: 2-D grids (unit-stride axis ax[1] with stages, several rows)
         h->rows_ok = h->plan.ax[2].n == 1 && h->plan.ax[0].n > 1 && h->plan.ax[1].nst > 0;
+        if (herm_planes && !(h->plane_cfg.persist && h->rows_ok))
+            return bail(fail(h, EDUS_ERR_UNSUPPORTED,
+                             "the Hermitian-plane form needs a 2-D grid whose plane fits the persistent plane "
+                             "kernel (at most 7040 k points)"));
     }
     if ((rc = set_smem(h, plane_rhs_kernel<true, kRadixAll, 512>, h->smem_plane))) return bail(rc);
     if ((rc = set_smem(h, plane_rhs_kernel<false, kRadixAll, 512>, h->smem_plane))) return bail(rc);
@@ -1318,6 +1337,14 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
             h->use3 = true;
         }
     }
+    std::vector<int> upair_host;
+    if (herm_planes) {
+        h->hplanes = true;
+        h->Pu = h->nb * (h->nb + 1) / 2;
+        for (int n = 0; n < h->nb; ++n)
+            for (int m = n; m < h->nb; ++m) upair_host.push_back(n * h->nb + m);
+        TRY_ALLOC(h->upair, upair_host.size() * sizeof(int));
+    }
     TRY_ALLOC(h->popbuf, h->nb * sizeof(double));
     TRY_ALLOC(h->flag, sizeof(int));
     if (cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream) != cudaSuccess)
@@ -1426,6 +1453,8 @@ int edus_create(const edus_desc* desc, edus_handle** out) {
     }
     if (cudaMemcpyAsync(h->roots, roots.data(), roots.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
         cudaMemcpyAsync(h->rpos, rpos.data(), rpos.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        (h->upair && cudaMemcpyAsync(h->upair, upair_host.data(), upair_host.size() * sizeof(int),
+                                     cudaMemcpyHostToDevice, h->stream) != cudaSuccess) ||
         cudaMemsetAsync(h->y, 0, SBb, h->stream) != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess)
         return bail(fail(h, EDUS_ERR_CUDA, "initial upload failed"));
     *out = h;
@@ -1485,7 +1514,8 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, co
         // forms cannot represent (e.g. two off-origin Wannier centres under
         // the cumulative r of ModelCoulomb.cpp:76-79).
         std::vector<double> Wuse;
-        if (h->packed) {
+        const bool herm_w = h->packed || h->hplanes;
+        if (herm_w) {
             const int nb = h->nb;
             Wuse.assign(h->S, 0.0);
             double mx = 0, dev = 0;
@@ -1509,7 +1539,7 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, co
                     }
             if (dev > 1e-12 * std::max(mx, 1e-300))
                 return fail(h, EDUS_ERR_UNSUPPORTED,
-                            "the packed forms need W_nm(R) = W_mn(-R) (Hermitian self-energy); this model's Wannier "
+                            "the Hermitian forms need W_nm(R) = W_mn(-R) (Hermitian self-energy); this model's Wannier "
                             "centres break it (use EDUS_PREC_FP64)");
         }
         std::vector<double> w(h->S);
@@ -1524,7 +1554,7 @@ int edus_upload_model(edus_handle* h, const double* H0_k, const double* xi_k, co
                         const double* wsrc = W_R + 2 * ((size_t)iR * P + p);
                         if (wsrc[1] != 0.0)
                             return fail(h, EDUS_ERR_ARG, "W_R must be real (the screened potential has no imaginary part)");
-                        w[(size_t)p * Nk + pos] = h->packed ? Wuse[(size_t)iR * P + p] : wsrc[0];
+                        w[(size_t)p * Nk + pos] = herm_w ? Wuse[(size_t)iR * P + p] : wsrc[0];
                         const double* rsrc = rho0_R + 2 * ((size_t)iR * P + p);
                         r0[(size_t)p * Nk + pos] = make_double2(rsrc[0], rsrc[1]);
                     }
@@ -1605,7 +1635,7 @@ int edus_set_kgradient(edus_handle* h, int n, const int* shift, const double* b,
         h->kg_n = 0;
         return EDUS_OK;
     }
-    if (h->packed || h->split)
+    if (h->packed || h->split || h->hplanes)
         return fail(h, EDUS_ERR_UNSUPPORTED, "gradient_space \"k\" is implemented for the FP64 form");
     if (n > 4096) return fail(h, EDUS_ERR_ARG, "k-gradient stencil longer than 4096 vectors");
     std::vector<int> sh(3 * (size_t)n);
@@ -1642,7 +1672,8 @@ int edus_set_peierls(edus_handle* h, int on) {
         return EDUS_OK;
     }
     if (!h->model_ready) return fail(h, EDUS_ERR_ARG, "edus_upload_model must be called first");
-    if (h->packed || h->split) return fail(h, EDUS_ERR_UNSUPPORTED, "the Peierls gauge is implemented for the FP64 form");
+    if (h->packed || h->split || h->hplanes)
+        return fail(h, EDUS_ERR_UNSUPPORTED, "the Peierls gauge is implemented for the FP64 form");
     if (h->per_solve) return fail(h, EDUS_ERR_UNSUPPORTED, "the Peierls gauge needs one model for all solves");
     if (h->nO > 0) return fail(h, EDUS_ERR_UNSUPPORTED, "the Peierls gauge does not combine with a Fock override");
     if (h->Nk * sizeof(double2) > (size_t)device_smem_optin(h->d.device))
@@ -2031,7 +2062,7 @@ struct FusedSweep {
 constexpr size_t kSweepSmallPlane = 110 * 1024;
 
 static bool fused_eligible(const edus_handle* h) {
-    return h->d.solver == EDUS_SOLVER_RK && !h->d.coulomb && !h->packed && !h->split && !h->peierls &&
+    return h->d.solver == EDUS_SOLVER_RK && !h->d.coulomb && !h->packed && !h->split && !h->hplanes && !h->peierls &&
            h->kg_n == 0 && !h->profiling;
 }
 

@@ -224,7 +224,14 @@ __global__ void __launch_bounds__(MAXT) plane_rhs_kernel(
 // only the ax[0] stages, which mix rows, are CTA-wide.  The arithmetic is the
 // same as without ROWS, in the same order, so the results are bitwise equal;
 // a plane then needs 9 CTA barriers instead of 16.
-template <bool COUL, int MASK, int MAXT, int BT = 1, bool ROWS = false>
+//
+// HERM (with ROWS; the Hermitian-plane form): only the band pairs n <= m are
+// transformed (upair[i] = n nb + m, nb (nb+1)/2 of them, nplanes = that times
+// the solves); G and H of the pair (m, n) are written as the conjugates of
+// those of (n, m).  That is the generator for Hermitian rho and H: exact for
+// the reference's on odd grids, and its Hermitian part on even ones (the host
+// gives the N/2 index coordinate 0 and symmetrises W, as for the packed forms).
+template <bool COUL, int MASK, int MAXT, int BT = 1, bool ROWS = false, bool HERM = false>
 __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     const double2* __restrict__ rho, long long batch_stride_in, double2* __restrict__ G_out,
     double2* __restrict__ Hee_out, long long batch_stride_out, const double2* __restrict__ rho0p,
@@ -233,7 +240,8 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     double2* __restrict__ scratch, int nplanes, const int* __restrict__ hpos, const double2* __restrict__ hval,
     int nS, const int* __restrict__ opos, const double2* __restrict__ oval, int nO,
     const double2* __restrict__ ptab = nullptr, int ntab = 0, int* status = nullptr, int wait_polls = 1 << 22,
-    int nroot_s = 0, int nrpos_s = 0) {
+    int nroot_s = 0, int nrpos_s = 0, const int* __restrict__ upair = nullptr) {
+    static_assert(!HERM || ROWS, "the Hermitian-plane form runs the row-wise kernel");
     extern __shared__ double2 smem[];
     const int Nk = pl.Nk;
     const int P = nb * nb;
@@ -275,8 +283,11 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
     for (int w = blockIdx.x; w < nplanes; w += gridDim.x) {
         // the solves of one band-pair plane run side by side: rho0 and W, which
         // they share, come from HBM once and from L2 for the others
-        const int nbat = nplanes / P;
-        const int p = w / nbat, b = w - (w / nbat) * nbat;
+        const int nbat = nplanes / (HERM ? nb * (nb + 1) / 2 : P);
+        const int pi = w / nbat, b = w - (w / nbat) * nbat;
+        const int p = HERM ? __ldg(&upair[pi]) : pi;
+        // HERM: the transposed pair, whose G and H are the conjugates
+        const int pT = (p - (p / nb) * nb) * nb + p / nb;
         if (!ROWS && ptab) {
             // Peierls gauge: no gradient term, two transforms (one without
             // HSEX); H = (H0 + E.xi + Hee[rho e^{-iA.R}]) e^{iA.R}
@@ -386,6 +397,14 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                 bulk_commit();
             }
         }
+        if (HERM && pT != p) {
+            // G of (m, n): the conjugate (reads of X beside the bulk store's)
+            double2* gT = G_out + (long long)b * batch_stride_out + (long long)pT * Nk;
+            for (int i = threadIdx.x; i < Nk; i += blockDim.x) {
+                const double2 v = X[i];
+                gT[i] = make_double2(v.x, -v.y);
+            }
+        }
         if (COUL) {
             if (bulk && threadIdx.x == 0) bulk_wait_read();
             __syncthreads();  // the store above has read X before it is refilled
@@ -469,6 +488,13 @@ __global__ void __launch_bounds__(MAXT, 2) plane_rhs_persist_kernel(
                         bulk_store((unsigned char*)hdst + off, (const unsigned char*)X + off,
                                    min(32768u, bytes - off));
                     bulk_commit();
+                }
+            }
+            if (HERM && pT != p) {
+                double2* hT = Hee_out + (long long)b * batch_stride_out + (long long)pT * Nk;
+                for (int i = threadIdx.x; i < Nk; i += blockDim.x) {
+                    const double2 v = X[i];
+                    hT[i] = make_double2(v.x, -v.y);
                 }
             }
         }

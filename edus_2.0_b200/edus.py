@@ -24,7 +24,7 @@ EDUS_OK = 0
 ERRORS = {1: "EDUS_ERR_ARG", 2: "EDUS_ERR_CUDA", 3: "EDUS_ERR_TIMEOUT", 4: "EDUS_ERR_DIVERGED",
           5: "EDUS_ERR_UNSUPPORTED", 6: "EDUS_ERR_NOMEM"}
 SOLVER_AB, SOLVER_RK = 0, 1
-PREC_FP64, PREC_HERM64, PREC_MIXED, PREC_SPLIT32 = 0, 1, 2, 3
+PREC_FP64, PREC_HERM64, PREC_MIXED, PREC_SPLIT32, PREC_HPLANES = 0, 1, 2, 3, 4
 ENVELOPE_SIN2, ENVELOPE_GAUSS = 0, 1
 
 # every entry point of include/edus_gpu.h

@@ -80,6 +80,18 @@ extern "C" {
  *          FP32, so their rounding scales with |delta|.  The commutator, the
  *          stage updates and the state are FP64. */
 #define EDUS_PREC_SPLIT32 3
+/*   HPLANES the FP64 form's state, commutators and stage updates, with the
+ *          k<->R transforms of the band pairs n <= m only: the gradient and
+ *          Hamiltonian planes of (m, n) are written as the conjugates of those
+ *          of (n, m), as they are for Hermitian rho and H.  On odd grids this
+ *          is the reference's generator (to rounding), with 48% fewer
+ *          transforms at 22 bands; on even grids it is the generator's
+ *          Hermitian part, as for HERM64 (coordinate 0 on the N/2 index, W
+ *          symmetrised; the upload refuses a W that is asymmetric elsewhere).
+ *          2-D grids of at most 7040 k points, length gauge, R-space
+ *          gradient; edus_rhs returns the Hermitian part of f for an input
+ *          that is not Hermitian. */
+#define EDUS_PREC_HPLANES 4
 
 /* Laser envelopes.  SIN2 is the reference's pulse (src/Laser/Laser.cpp:96-134):
  *   E(t) = sqrt(I) sin^2(pi (t-t0)/(cycles*T)) sin(w (t-t0) + phase) pol,
@@ -99,7 +111,7 @@ typedef struct {
     int order;       /* 4 for RK; 4 or 5 for AB */
     double dt;       /* DESolver::ResolutionTime, a.u. */
     int coulomb;     /* 1: add the HSEX self-energy (Coulomb::EffectiveHamiltonian) */
-    int precision;   /* EDUS_PREC_FP64, _HERM64, _MIXED or _SPLIT32 */
+    int precision;   /* EDUS_PREC_FP64, _HERM64, _MIXED, _SPLIT32 or _HPLANES */
     int batch;       /* independent solves sharing one model (>= 1) */
     int device;      /* CUDA device ordinal */
 } edus_desc;
