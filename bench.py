@@ -211,6 +211,21 @@ def _trajectory(s, b, vel, nsteps, every, filled):
     return np.array(J).T, rhos
 
 
+def best_form(forms, batched_rate, single_rate):
+    """The fastest form within 1e-8 of plain FP64 (per-GPU rates; the batched
+    FP64 rate is the timed value's) and its ratio over one plain FP64 solve."""
+    cand = [("batched FP64", batched_rate)]
+    bh = forms.get("batched_hplanes", {})
+    if bh.get("meets_1e-8"):
+        cand.append(("batched HPLANES", bh["solve_steps_per_s"]))
+    for name, _ in FORMS:
+        f = forms.get(name, {})
+        if f.get("meets_1e-8"):
+            cand.append((name, f["steps_per_s"]))
+    name, rate = max(cand, key=lambda c: c[1])
+    return {"form": name, "steps_per_s": round(rate, 1), "vs_fp64_ratio": round(rate / single_rate, 4)}
+
+
 def accuracy_and_forms(pkg, model, cfg, B, laser_of, nsteps, timed_steps, torch):
     """Each form against plain FP64 on the workload from t = 0: max |rho -
     rho_FP64| over 10 checkpoints of an `nsteps`-step run, and the relative
@@ -238,15 +253,8 @@ def accuracy_and_forms(pkg, model, cfg, B, laser_of, nsteps, timed_steps, torch)
     sb.close()
     d, h = compare(Jb, rb)
     out["batched_fp64"] = {"max_abs_drho": d, "hhg_rel_err": h}
-    for name, const in FORMS:
-        try:
-            s = model.solver(batch=1, precision=getattr(E, const))
-        except E.EdusError as e:
-            out[name] = {"unavailable": str(e)}
-            continue
-        J, rhos = _trajectory(s, 0, vel, nsteps, every, cfg.filledbands)
-        d, h = compare(J, rhos)
-        # speed: device time of timed_steps steps without observables
+
+    def timed(s, nsol):
         st = torch.cuda.ExternalStream(s.stream)
         s.step(3)
         s.synchronize()
@@ -256,8 +264,30 @@ def accuracy_and_forms(pkg, model, cfg, B, laser_of, nsteps, timed_steps, torch)
         e1.record(st)
         s.synchronize()
         torch.cuda.synchronize()
-        out[name] = {"steps_per_s": round(timed_steps / (e0.elapsed_time(e1) / 1e3), 1), "max_abs_drho": d,
-                     "hhg_rel_err": h, "meets_1e-8": bool(d <= 1e-8)}
+        return round(nsol * timed_steps / (e0.elapsed_time(e1) / 1e3), 1)
+
+    # the Hermitian-plane form with the batch (solve 0 under the workload's pulse)
+    try:
+        sh = model.solver(batch=B, precision=E.PREC_HPLANES)
+        for b in range(B):
+            sh.set_lasers([laser_of(b)], b)
+        Jh, rh = _trajectory(sh, 0, vel, nsteps, every, cfg.filledbands)
+        d, h = compare(Jh, rh)
+        out["batched_hplanes"] = {"solve_steps_per_s": timed(sh, B), "max_abs_drho": d, "hhg_rel_err": h,
+                                  "meets_1e-8": bool(d <= 1e-8)}
+        sh.close()
+    except E.EdusError as e:
+        out["batched_hplanes"] = {"unavailable": str(e)}
+    for name, const in FORMS:
+        try:
+            s = model.solver(batch=1, precision=getattr(E, const))
+        except E.EdusError as e:
+            out[name] = {"unavailable": str(e)}
+            continue
+        J, rhos = _trajectory(s, 0, vel, nsteps, every, cfg.filledbands)
+        d, h = compare(J, rhos)
+        # speed: device time of timed_steps steps without observables
+        out[name] = {"steps_per_s": timed(s, 1), "max_abs_drho": d, "hhg_rel_err": h, "meets_1e-8": bool(d <= 1e-8)}
         s.close()
     return out
 
@@ -421,13 +451,14 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(ms_max / K, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "form": (f"batched FP64: {B} solves per launch on the drop-in FP64 kernels (the fastest form within "
-                 f"1e-8 of plain FP64 on this workload; reduced-precision forms in `forms`)"),
+        "form": (f"batched FP64: {B} solves per launch on the drop-in FP64 kernels (the timed value; "
+                 f"`best_form` names the fastest form within 1e-8 of plain FP64 among those in `forms`)"),
         "single_solve_steps_per_s": round(single, 3),
         "vs_fp64_ratio": round(value / world / single, 4),
         "max_abs_drho": forms["batched_fp64"]["max_abs_drho"] if forms else None,
         "hhg_rel_err": forms["batched_fp64"]["hhg_rel_err"] if forms else None,
         "forms": forms,
+        "best_form": best_form(forms, value / world, single) if forms else None,
         "config": {"workload": f"{WORKLOAD}: 22-orbital TMD-like, {GRID[0]}x{GRID[1]}x1 k grid, HSEX (RK r0=40 A, eps=1), "
                                f"RK4 dt=0.005 fs, batch={B} solve(s) per GPU (laser intensity x(1 + b/4))",
                    "batch": B, "l2": f"inputs larger than L2 (state {S_bytes / 1e6:.1f} MB x {B}; "
