@@ -322,7 +322,8 @@ def run_ours(args, rank, world, local_rank):
             torch.distributed.barrier()
 
     # single-solve rate (reported beside the batched value)
-    s1 = model.solver(batch=1, device=local_rank)
+    prec = pkg.edus.PREC_HPLANES if args.form == "hplanes" else pkg.edus.PREC_FP64
+    s1 = model.solver(batch=1, device=local_rank, precision=prec)
     s1.time = t_start
     for _ in range(args.warmup):
         s1.step(1)
@@ -339,7 +340,7 @@ def run_ours(args, rank, world, local_rank):
     del s1
 
     # the batch: a laser-amplitude sweep, solve b at (1 + b/4) times the intensity
-    s = model.solver(batch=B, device=local_rank)
+    s = model.solver(batch=B, device=local_rank, precision=prec)
     base = cfg.lasers[0]
     for b in range(B):
         s.set_lasers([pkg.Laser(base.intensity * (1.0 + 0.25 * b), base.omega, base.pol, base.cycles, base.t0,
@@ -451,8 +452,10 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": round(value, 3), "unit": "steps/s", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(ms_max / K, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "form": (f"batched FP64: {B} solves per launch on the drop-in FP64 kernels (the timed value; "
-                 f"`best_form` names the fastest form within 1e-8 of plain FP64 among those in `forms`)"),
+        "form": ((f"batched FP64: {B} solves per launch on the drop-in FP64 kernels (the timed value; "
+                  f"`best_form` names the fastest form within 1e-8 of plain FP64 among those in `forms`)")
+                 if args.form == "fp64" else
+                 f"batched HPLANES: {B} solves per launch, transforms of the band pairs n <= m only"),
         "single_solve_steps_per_s": round(single, 3),
         "vs_fp64_ratio": round(value / world / single, 4),
         "max_abs_drho": forms["batched_fp64"]["max_abs_drho"] if forms else None,
@@ -826,6 +829,8 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=4000)
     ap.add_argument("--workload", choices=["tmd22_rk4", "sweep", "surrogate"], default="tmd22_rk4")
     ap.add_argument("--grid", type=int, default=72, help="tmd22_rk4: N for the N x N k grid (72: the benchmark)")
+    ap.add_argument("--form", choices=["fp64", "hplanes"], default="fp64",
+                    help="tmd22_rk4: the form of the timed loop (fp64: the drop-in)")
     ap.add_argument("--surrogate-snapshots", type=int, default=2000)
     ap.add_argument("--surrogate-run-steps", type=int, default=2000)
     ap.add_argument("--surrogate-iters", type=int, default=3000)
